@@ -1,0 +1,156 @@
+/*
+ * sles.h -- C ABI of the B200 spectral-LES library (libsles_b200.so).
+ *
+ * The reference (a-k-sangwan/spectral-LES) is pure Python; its hot path is
+ * a set of functions that mutate an ``InitializeDomain`` attribute bag.  This
+ * library replaces the arithmetic of those functions; the Python package
+ * ``sles`` (spectral-les_b200/sles) keeps the reference's call surface and
+ * calls these entry points through ctypes.  Each declaration names the
+ * reference code it replaces (path:line inside the reference repository).
+ *
+ * Conventions
+ *  - All pointers are device pointers unless stated; fields use the layouts
+ *    documented in sles_layout below.  No torch or C++ types cross the ABI.
+ *  - Every call takes an explicit cudaStream_t (passed as void*), enqueues
+ *    work and returns without synchronising, except where stated.
+ *  - Return value: SLES_OK (0) or a positive SLES_ERR_* code; nothing throws.
+ *  - No entry point allocates device memory on the hot path: intermediate
+ *    fields live in a caller-provided workspace (sles_plan_workspace_bytes).
+ *  - A plan is not thread-safe; use one stream per plan.
+ */
+#ifndef SLES_H
+#define SLES_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SLES_VERSION 1
+
+enum sles_status {
+  SLES_OK = 0,
+  SLES_ERR_INVALID_ARG = 1,     /* null pointer, bad enum, inconsistent sizes       */
+  SLES_ERR_UNSUPPORTED = 2,     /* grid size / combination without a compiled kernel */
+  SLES_ERR_CUDA = 3,            /* a CUDA runtime call failed                        */
+  SLES_ERR_WORKSPACE = 4,       /* workspace missing or smaller than required        */
+  SLES_ERR_TIMEOUT = 5,         /* a bounded device-side wait gave up                */
+  SLES_ERR_NONFINITE = 6,       /* a reduction saw NaN/Inf (reference: dt != dt)     */
+  SLES_ERR_STATE = 7            /* call out of order (e.g. ETD2 step before bootstrap) */
+};
+
+enum sles_dtype { SLES_F32 = 0, SLES_F64 = 1 };
+enum sles_les_model { SLES_LES_NONE = 0, SLES_LES_SMAGORINSKY = 1, SLES_LES_VREMAN = 2 };
+enum sles_scheme { SLES_RK4 = 0, SLES_RK3 = 1, SLES_ETD2 = 2 };
+
+/*
+ * Plan descriptor.  Mirrors InitializeDomain(nu, dimension, No_of_gridpoint,
+ * forcing, method, LES_ON, Cs, LES_model) (src/initialize_domain.py:20-33).
+ * ``n`` is the computational grid (the reference divides No_of_gridpoint by 4
+ * when LES is on, src/initialize_domain.py:38-40; the Python layer applies it).
+ */
+typedef struct sles_plan_desc {
+  int dim;          /* 2 or 3 */
+  int n;            /* grid points per axis: 16,24,32,48,64,96,128,256,512 (3D); up to 1024 (2D) */
+  int dtype;        /* enum sles_dtype: arithmetic of the fields and transforms */
+  int les_model;    /* enum sles_les_model */
+  int scheme;       /* enum sles_scheme */
+  int parity;       /* 1: the reference's arithmetic including its quirks; 0: corrected schemes */
+  double nu;        /* kinematic viscosity */
+  double cs;        /* Smagorinsky / Vreman constant */
+  double forcing;   /* linear forcing coefficient (src/RK4_method.py:58-64) */
+} sles_plan_desc;
+
+typedef struct sles_plan sles_plan;
+
+/* Field layout numbers for a plan: elements per half-complex field (complex
+ * count, rows padded to nkp), per real field, and the padded row length. */
+typedef struct sles_layout {
+  int64_t hc_elems;     /* N*N*nkp (3D) or N*nkp (2D) complex elements */
+  int64_t real_elems;   /* N^dim real elements */
+  int32_t nkp;          /* padded length of a half-complex row (>= N/2+1) */
+  int32_t nk;           /* N/2 + 1 */
+} sles_layout;
+
+/* Build a plan (replaces the PFFT plan + wavenumber/mask set-up,
+ * src/initialize_domain.py:59-65, 76-114, 162-167).  No device allocation. */
+int sles_plan_create(const sles_plan_desc* desc, sles_plan** out);
+int sles_plan_destroy(sles_plan* plan);
+int sles_plan_layout(const sles_plan* plan, sles_layout* out);
+/* Bytes of device workspace the plan needs for intermediate fields. */
+size_t sles_plan_workspace_bytes(const sles_plan* plan);
+/* Attach caller-owned device workspace (>= sles_plan_workspace_bytes). */
+int sles_plan_set_workspace(sles_plan* plan, void* ws, size_t bytes);
+/* Update run-time scalars (nu, cs, forcing) without rebuilding. */
+int sles_plan_set_params(sles_plan* plan, double nu, double cs, double forcing);
+
+/* Batched unscaled r2c over the last ``dim`` axes: PFFT.forward(normalize=False)
+ * (src/math_formula.py:7-12, src/initial.py:13).  real_in: nfields real
+ * fields; hc_out: nfields half-complex fields. */
+int sles_fft_r2c(sles_plan* plan, const void* real_in, void* hc_out, int nfields, void* stream);
+/* Batched c2r scaled by 1/N^dim: PFFT.backward(normalize=True)
+ * (src/math_formula.py:18-24, src/RK4_method.py:32-34).  Uses the workspace;
+ * hc_in is not modified. */
+int sles_fft_c2r(sles_plan* plan, const void* hc_in, void* real_out, int nfields, void* stream);
+
+/* Physical velocity and vorticity from U_hat: U = irfftn(U_hat) and
+ * curl = irfftn(i k x U_hat) (src/RK4_method.py:28-34, src/math_formula.py:16-25).
+ * curl has 3 fields in 3D, 1 in 2D.  Either output may be NULL. */
+int sles_velocity_curl(sles_plan* plan, const void* u_hat, void* u_out, void* curl_out, void* stream);
+
+/* Velocity gradient a[i][j] = d u_j / d x_i = irfftn(i K_i U_hat_j) as dim*dim
+ * real fields in row-major (i, j) order (src/math_formula.py:27-62). */
+int sles_velocity_gradient(sles_plan* plan, const void* u_hat, void* grad_out, void* stream);
+
+/*
+ * One right-hand-side evaluation, fused: dU = P(mask*rfftn(u x omega) + T_hat)
+ * [+ f U_hat] - nu K^2 U_hat (src/RK4_method.py:38-71 == src/RK3_method.py:44-77,
+ * with Smagorinsky_model / Vreman_model, src/smagorinsky.py:8-47,
+ * src/vreman.py:8-123, and residue_stress, src/math_formula.py:64-127).
+ * u_phys / curl_phys: optional physical fields used instead of the ones
+ * implied by u_hat (the reference's stage 0 reuses the stored U and curl,
+ * src/RK4_method.py:39-47); pass NULL to derive them from u_hat.
+ * f1_out (optional): the projected term before the viscous term and before
+ * T_hat is added back (the reference's ETD2 F1, src/RK4_method.py:65-66).
+ */
+int sles_rhs(sles_plan* plan, const void* u_hat, const void* u_phys, const void* curl_phys,
+             void* du_out, void* f1_out, void* stream);
+
+/*
+ * One integrator stage, fused with the right-hand side it needs.
+ * Replaces the bodies of RK4.solveForNextTimestep (src/RK4_method.py:20-35),
+ * RK3.solveForNextTimestep (src/RK3_method.py:20-41) and
+ * ETD2.solveForNextTimestep (src/ETD2_method.py:7-37).
+ *   u_cur   : U_hat the RHS is evaluated at (read)
+ *   u0      : U_hat at the start of the step (read; RK stages)
+ *   u1      : RK4 accumulator U_hat1 (read+write); ETD2: F1 of the previous step (read)
+ *   u_out   : new U_hat (write; may alias u_cur)
+ *   aux_out : RK4 last stage: second copy of the result; ETD2: new F1 (write)
+ * stage: RK4 0..3, RK3 0..2, ETD2 0.  dt: step size.  u_phys / curl_phys as in
+ * sles_rhs.  flags: SLES_STAGE_* below.
+ */
+enum { SLES_STAGE_RECORD_F1 = 1 };
+int sles_stage(sles_plan* plan, int stage, double dt, const void* u_cur, const void* u0, void* u1,
+               void* u_out, void* aux_out, const void* u_phys, const void* curl_phys, int flags,
+               void* stream);
+
+/*
+ * Diagnostics from U_hat, accumulated in float64 with compensated sums:
+ * out[0] = E = 1/2 <u.u>, out[1] = eps = nu <|grad u|^2>, out[2] = max_i max_x u_i
+ * (signed, as find_max_velocity, src/SM_solver.py:245-255; needs u_phys),
+ * out[3] = nonfinite flag.  spectrum (optional, nshell doubles): E(k) on
+ * integer shells round(|k|).  out and spectrum are DEVICE pointers.
+ */
+int sles_diag(sles_plan* plan, const void* u_hat, const void* u_phys, double* out, double* spectrum,
+              int nshell, void* stream);
+
+/* Human-readable text for a status code (static storage). */
+const char* sles_status_string(int status);
+int sles_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SLES_H */

@@ -1,0 +1,182 @@
+// C ABI of libsles_b200.so (declarations and reference citations: include/sles.h).
+#include <cstdio>
+#include <new>
+
+#include "sles_engine.cuh"
+
+namespace sles {
+#define SLES_DECL(NN) Engine* make_engine_##NN(int dtype, int dim);
+SLES_DECL(16) SLES_DECL(24) SLES_DECL(32) SLES_DECL(48) SLES_DECL(64) SLES_DECL(96) SLES_DECL(128)
+SLES_DECL(256) SLES_DECL(512) SLES_DECL(1024)
+#undef SLES_DECL
+
+Engine* make_engine(int dtype, int dim, int n) {
+  switch (n) {
+    case 16: return make_engine_16(dtype, dim);
+    case 24: return make_engine_24(dtype, dim);
+    case 32: return make_engine_32(dtype, dim);
+    case 48: return make_engine_48(dtype, dim);
+    case 64: return make_engine_64(dtype, dim);
+    case 96: return make_engine_96(dtype, dim);
+    case 128: return make_engine_128(dtype, dim);
+    case 256: return make_engine_256(dtype, dim);
+    case 512: return make_engine_512(dtype, dim);
+    case 1024: return make_engine_1024(dtype, dim);
+    default: return nullptr;
+  }
+}
+}  // namespace sles
+
+struct sles_plan {
+  sles::PlanInfo info;
+  sles::Engine* eng;
+};
+
+
+
+extern "C" {
+
+int sles_version(void) { return SLES_VERSION; }
+
+const char* sles_status_string(int s) {
+  switch (s) {
+    case SLES_OK: return "ok";
+    case SLES_ERR_INVALID_ARG: return "invalid argument";
+    case SLES_ERR_UNSUPPORTED: return "unsupported grid size or combination";
+    case SLES_ERR_CUDA: return "CUDA runtime error";
+    case SLES_ERR_WORKSPACE: return "workspace missing or too small";
+    case SLES_ERR_TIMEOUT: return "bounded device wait timed out";
+    case SLES_ERR_NONFINITE: return "non-finite value";
+    case SLES_ERR_STATE: return "call out of order";
+    default: return "unknown status";
+  }
+}
+
+int sles_plan_create(const sles_plan_desc* d, sles_plan** out) {
+  if (!d || !out) return SLES_ERR_INVALID_ARG;
+  *out = nullptr;
+  if ((d->dim != 2 && d->dim != 3) || (d->dtype != SLES_F32 && d->dtype != SLES_F64)) return SLES_ERR_INVALID_ARG;
+  if (d->les_model < SLES_LES_NONE || d->les_model > SLES_LES_VREMAN) return SLES_ERR_INVALID_ARG;
+  if (d->scheme < SLES_RK4 || d->scheme > SLES_ETD2) return SLES_ERR_INVALID_ARG;
+  if (d->parity != 0 && d->parity != 1) return SLES_ERR_INVALID_ARG;
+  if (!(d->nu >= 0.0) || !(d->forcing >= 0.0)) return SLES_ERR_INVALID_ARG;
+  sles::Engine* eng = sles::make_engine(d->dtype, d->dim, d->n);
+  if (!eng) return SLES_ERR_UNSUPPORTED;
+  sles_plan* p = new (std::nothrow) sles_plan();
+  if (!p) {
+    delete eng;
+    return SLES_ERR_INVALID_ARG;
+  }
+  p->eng = eng;
+  sles::PlanInfo& I = p->info;
+  I.d = *d;
+  I.nk = d->n / 2 + 1;
+  I.nkp = (I.nk + 3) / 4 * 4;
+  I.hc_elems = (long long)(d->dim == 3 ? d->n * d->n : d->n) * I.nkp;
+  I.real_elems = (long long)d->n * d->n * (d->dim == 3 ? d->n : 1);
+  I.elem_bytes = d->dtype == SLES_F32 ? 8 : 16;
+  I.ws = nullptr;
+  I.ws_bytes = 0;
+  I.ws_fields = eng->ws_fields_needed(I);
+  I.flags = nullptr;
+  I.scal = nullptr;
+  *out = p;
+  return SLES_OK;
+}
+
+int sles_plan_destroy(sles_plan* p) {
+  if (!p) return SLES_ERR_INVALID_ARG;
+  delete p->eng;
+  delete p;
+  return SLES_OK;
+}
+
+int sles_plan_layout(const sles_plan* p, sles_layout* out) {
+  if (!p || !out) return SLES_ERR_INVALID_ARG;
+  out->hc_elems = p->info.hc_elems;
+  out->real_elems = p->info.real_elems;
+  out->nkp = p->info.nkp;
+  out->nk = p->info.nk;
+  return SLES_OK;
+}
+
+size_t sles_plan_workspace_bytes(const sles_plan* p) {
+  if (!p) return 0;
+  const sles::PlanInfo& I = p->info;
+  return sles::slots_offset(I.d.dim, I.d.n) + (size_t)I.ws_fields * I.hc_elems * I.elem_bytes;
+}
+
+int sles_plan_set_workspace(sles_plan* p, void* ws, size_t bytes) {
+  if (!p) return SLES_ERR_INVALID_ARG;
+  if (!ws || bytes < sles_plan_workspace_bytes(p)) return SLES_ERR_WORKSPACE;
+  if (((uintptr_t)ws) % 256 != 0) return SLES_ERR_INVALID_ARG;
+  p->info.ws = ws;
+  p->info.ws_bytes = bytes;
+  p->info.flags = reinterpret_cast<unsigned*>(ws);
+  p->info.scal = reinterpret_cast<double*>(reinterpret_cast<char*>(ws) + 256);
+  return SLES_OK;
+}
+
+int sles_plan_set_params(sles_plan* p, double nu, double cs, double forcing) {
+  if (!p || !(nu >= 0.0) || !(forcing >= 0.0)) return SLES_ERR_INVALID_ARG;
+  p->info.d.nu = nu;
+  p->info.d.cs = cs;
+  p->info.d.forcing = forcing;
+  return SLES_OK;
+}
+
+static int ready(sles_plan* p) {
+  if (!p) return SLES_ERR_INVALID_ARG;
+  if (!p->info.ws) return SLES_ERR_WORKSPACE;
+  return SLES_OK;
+}
+
+int sles_fft_r2c(sles_plan* p, const void* in, void* out, int nf, void* stream) {
+  if (int s = ready(p)) return s;
+  if (!in || !out || nf < 0) return SLES_ERR_INVALID_ARG;
+  return p->eng->fft_r2c(p->info, in, out, nf, (cudaStream_t)stream);
+}
+
+int sles_fft_c2r(sles_plan* p, const void* in, void* out, int nf, void* stream) {
+  if (int s = ready(p)) return s;
+  if (!in || !out || nf < 0) return SLES_ERR_INVALID_ARG;
+  return p->eng->fft_c2r(p->info, in, out, nf, (cudaStream_t)stream);
+}
+
+int sles_velocity_curl(sles_plan* p, const void* uh, void* u, void* curl, void* stream) {
+  if (int s = ready(p)) return s;
+  if (!uh) return SLES_ERR_INVALID_ARG;
+  return p->eng->velocity_curl(p->info, uh, u, curl, (cudaStream_t)stream);
+}
+
+int sles_velocity_gradient(sles_plan* p, const void* uh, void* grad, void* stream) {
+  if (int s = ready(p)) return s;
+  if (!uh || !grad) return SLES_ERR_INVALID_ARG;
+  return p->eng->velocity_gradient(p->info, uh, grad, (cudaStream_t)stream);
+}
+
+int sles_rhs(sles_plan* p, const void* uh, const void* uphys, const void* cphys, void* du, void* f1, void* stream) {
+  if (int s = ready(p)) return s;
+  if (!uh || !du) return SLES_ERR_INVALID_ARG;
+  if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
+  return p->eng->rhs(p->info, uh, uphys, cphys, du, f1, (cudaStream_t)stream);
+}
+
+int sles_stage(sles_plan* p, int stage, double dt, const void* ucur, const void* u0, void* u1, void* uout, void* aux,
+               const void* uphys, const void* cphys, int flags, void* stream) {
+  if (int s = ready(p)) return s;
+  if (!ucur || !uout || !(dt == dt)) return SLES_ERR_INVALID_ARG;
+  if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
+  const int scheme = (flags & sles::STAGE_RK4) ? SLES_RK4 : p->info.d.scheme;
+  if ((scheme == SLES_RK4 && (!u0 || !u1)) || (scheme == SLES_RK3 && !u0)) return SLES_ERR_INVALID_ARG;
+  return p->eng->stage(p->info, stage, dt, ucur, u0, u1, uout, aux, uphys, cphys, flags, (cudaStream_t)stream);
+}
+
+int sles_diag(sles_plan* p, const void* uh, const void* uphys, double* out, double* spectrum, int nshell,
+              void* stream) {
+  if (int s = ready(p)) return s;
+  if (!uh || !out || nshell < 0) return SLES_ERR_INVALID_ARG;
+  return p->eng->diag(p->info, uh, uphys, out, spectrum, nshell, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,418 @@
+// Host-side engine: launch sequences for one (precision, N, dim) triple.
+// One instantiation per grid size lives in sles_n<N>.cu so the sizes compile
+// in parallel; sles_api.cu dispatches to them through the Engine interface.
+#pragma once
+#include <cuda_runtime.h>
+#include <mutex>
+#include <unordered_set>
+
+#include "../../include/sles.h"
+#include "sles_misc.cuh"
+#include "sles_passes.cuh"
+#include "sles_rhs.cuh"
+
+namespace sles {
+
+struct PlanInfo {
+  sles_plan_desc d;
+  int nkp, nk;
+  long long hc_elems, real_elems;
+  size_t elem_bytes;     // bytes of one complex element
+  void* ws;              // workspace base (device)
+  size_t ws_bytes;
+  int ws_fields;         // half-complex field slots in the workspace
+  unsigned* flags;       // device error word inside the workspace
+  double* scal;          // device scalar scratch inside the workspace (64 doubles)
+};
+
+// workspace header: error word + scalar scratch, then the diagnostics area,
+// then the field slots (256-byte aligned)
+constexpr size_t WS_HEADER = 4096;
+inline int max_shell(int dim, int n) { return (int)(0.5 * n * (dim == 3 ? 1.7320508075688772 : 1.4142135623730951)) + 3; }
+inline size_t diag_area_bytes(int dim, int n) {
+  return ((size_t)DIAG_BLOCKS * (2 + max_shell(dim, n)) + DIAG_BLOCKS) * sizeof(double);
+}
+inline size_t slots_offset(int dim, int n) { return ((WS_HEADER + diag_area_bytes(dim, n)) + 255) / 256 * 256; }
+
+struct Engine {
+  virtual ~Engine() {}
+  virtual int ws_fields_needed(const PlanInfo& p) const = 0;
+  virtual int fft_r2c(PlanInfo& p, const void* in, void* out, int nf, cudaStream_t st) = 0;
+  virtual int fft_c2r(PlanInfo& p, const void* in, void* out, int nf, cudaStream_t st) = 0;
+  virtual int velocity_curl(PlanInfo& p, const void* uh, void* u, void* curl, cudaStream_t st) = 0;
+  virtual int velocity_gradient(PlanInfo& p, const void* uh, void* grad, cudaStream_t st) = 0;
+  virtual int rhs(PlanInfo& p, const void* uh, const void* uphys, const void* cphys, void* du, void* f1,
+                  cudaStream_t st) = 0;
+  virtual int stage(PlanInfo& p, int stage, double dt, const void* ucur, const void* u0, void* u1,
+                    void* uout, void* aux, const void* uphys, const void* cphys, int flags,
+                    cudaStream_t st) = 0;
+  virtual int diag(PlanInfo& p, const void* uh, const void* uphys, double* out, double* spec, int nshell,
+                   cudaStream_t st) = 0;
+};
+
+inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? SLES_OK : SLES_ERR_CUDA; }
+
+// Raise the dynamic shared-memory limit of a kernel once, then launch.
+template <typename... KArgs, typename... Args>
+inline int launch(void (*kern)(KArgs...), long long grid, int block, size_t smem, cudaStream_t st,
+                  Args... args) {
+  if (grid <= 0) return SLES_OK;
+  if (grid > 0x7fffffffLL) return SLES_ERR_UNSUPPORTED;
+  if (smem > 48 * 1024) {
+    static std::mutex mu;
+    static std::unordered_set<const void*> done;
+    std::lock_guard<std::mutex> g(mu);
+    if (!done.count((const void*)kern)) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return SLES_ERR_CUDA;
+      done.insert((const void*)kern);
+    }
+  }
+  kern<<<(unsigned)grid, block, smem, st>>>(static_cast<KArgs>(args)...);
+  return cuda_status(cudaGetLastError());
+}
+
+#define SLES_TRY(x)              \
+  do {                           \
+    int _s = (x);                \
+    if (_s != SLES_OK) return _s; \
+  } while (0)
+
+// columns per c2c work item: 64-byte row segments
+template <typename Tp> struct Cols { static constexpr int W = (sizeof(Tp) == 4) ? 8 : 4; };
+
+template <typename Tp, int N>
+struct Geo {
+  static constexpr int W = Cols<Tp>::W;
+  static constexpr int T = PlanFor<Tp, N>::F::T;
+  static constexpr int G = (W * T >= 256) ? 1 : 256 / (W * T);
+  static constexpr int TR = PlanFor<Tp, N / 2>::F::T;
+  static constexpr int LPB = (TR >= 128) ? 1 : 128 / TR;
+};
+
+// ---------------------------------------------------------------------------
+// standalone transforms
+// ---------------------------------------------------------------------------
+template <typename Tp, int N, int DIM>
+struct Transforms {
+  using C = typename CT<Tp>::C;
+  using G = Geo<Tp, N>;
+
+  // c2c along axis `ax` (0 = x, 1 = y; 2D: ax 0 only) of nf fields
+  template <int DIR>
+  static int c2c(const PlanInfo& p, const C* src, C* dst, int nf, int ax, Tp scale, cudaStream_t st) {
+    using K = C2CAxis<Tp, N, G::W, G::G>;
+    const long long fs = p.hc_elems;
+    const int nchunks = (p.nk + G::W - 1) / G::W;
+    int na;
+    long long astride, pstride;
+    if (DIM == 3) {
+      na = N;
+      if (ax == 0) { astride = p.nkp; pstride = (long long)N * p.nkp; }
+      else { astride = (long long)N * p.nkp; pstride = p.nkp; }
+    } else {
+      na = 1; astride = 0; pstride = p.nkp;
+    }
+    const long long items = (long long)nf * na * nchunks;
+    return launch(k_c2c_axis<Tp, N, G::W, G::G, DIR>, (items + G::G - 1) / G::G, K::THREADS, K::SMEM, st,
+                  src, dst, fs, nf, na, astride, pstride, p.nk, nchunks, scale);
+  }
+
+  static int r2c_lines(const PlanInfo& p, const Tp* src, C* dst, int nf, cudaStream_t st) {
+    using K = RealAxis<Tp, N, G::LPB>;
+    const long long nlines = (long long)nf * (DIM == 3 ? (long long)N * N : N);
+    return launch(k_r2c_line<Tp, N, G::LPB>, (nlines + G::LPB - 1) / G::LPB, K::THREADS, K::SMEM, st, src,
+                  dst, nlines, p.nkp);
+  }
+
+  static int c2r_lines(const PlanInfo& p, const C* src, Tp* dst, int nf, Tp scale, cudaStream_t st) {
+    using K = RealAxis<Tp, N, G::LPB>;
+    const long long nlines = (long long)nf * (DIM == 3 ? (long long)N * N : N);
+    return launch(k_c2r_line<Tp, N, G::LPB>, (nlines + G::LPB - 1) / G::LPB, K::THREADS, K::SMEM, st, src,
+                  dst, nlines, p.nkp, scale);
+  }
+
+  static int r2c(const PlanInfo& p, const Tp* in, C* out, int nf, cudaStream_t st) {
+    SLES_TRY(r2c_lines(p, in, out, nf, st));
+    if (DIM == 3) SLES_TRY(c2c<-1>(p, out, out, nf, 1, (Tp)1, st));
+    return c2c<-1>(p, out, out, nf, 0, (Tp)1, st);
+  }
+
+  // c2r of nf fields through `tmp` (nf half-complex slots); `in` is preserved
+  static int c2r(const PlanInfo& p, const C* in, Tp* out, int nf, C* tmp, cudaStream_t st) {
+    const Tp scale = (Tp)(1.0 / ((DIM == 3) ? (double)N * N * N : (double)N * N));
+    SLES_TRY(c2c<+1>(p, in, tmp, nf, 0, (Tp)1, st));
+    if (DIM == 3) SLES_TRY(c2c<+1>(p, tmp, tmp, nf, 1, (Tp)1, st));
+    return c2r_lines(p, tmp, out, nf, scale, st);
+  }
+};
+
+}  // namespace sles
+
+namespace sles {
+
+enum { STAGE_RECORD_F1 = 1, STAGE_PRIMED = 2, STAGE_NO_PREPARE = 4, STAGE_RK4 = 8 };
+
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+template <typename Tp, int N, int DIM>
+struct EngineImpl final : Engine {
+  using C = typename CT<Tp>::C;
+  using TR = Transforms<Tp, N, DIM>;
+  using FX = typename PlanLo<Tp, N>::F;
+  using FY = typename PlanFor<Tp, N>::F;
+  static constexpr int W = Cols<Tp>::W;
+  static constexpr int GX = cmax(1, 256 / (W * FX::T));
+  static constexpr int GY = cmax(1, 256 / (W * FY::T));
+  static constexpr int TZ = PlanFor<Tp, N / 2>::F::T;
+  static constexpr int LPI = cmax(1, 16 / TZ);
+
+  static C* slot(const PlanInfo& p, int i) {
+    return reinterpret_cast<C*>(reinterpret_cast<char*>(p.ws) + slots_offset(DIM, N)) + (long long)i * p.hc_elems;
+  }
+  static int nchunks(const PlanInfo& p) { return (p.nk + W - 1) / W; }
+
+  int ws_fields_needed(const PlanInfo& p) const override {
+    const bool les = p.d.les_model != SLES_LES_NONE;
+    if (DIM == 3) return les ? 9 : 6;
+    return les ? 5 : 3;
+  }
+
+  // ---------------- standalone transforms ----------------
+  int fft_r2c(PlanInfo& p, const void* in, void* out, int nf, cudaStream_t st) override {
+    return TR::r2c(p, (const Tp*)in, (C*)out, nf, st);
+  }
+  int fft_c2r(PlanInfo& p, const void* in, void* out, int nf, cudaStream_t st) override {
+    const int cap = p.ws_fields;
+    for (int f0 = 0; f0 < nf; f0 += cap) {
+      const int n = (nf - f0 < cap) ? nf - f0 : cap;
+      SLES_TRY(TR::c2r(p, (const C*)in + (long long)f0 * p.hc_elems, (Tp*)out + (long long)f0 * p.real_elems, n,
+                       slot(p, 0), st));
+    }
+    return SLES_OK;
+  }
+  int velocity_curl(PlanInfo& p, const void* uh, void* u, void* curl, cudaStream_t st) override {
+    if (u) SLES_TRY(fft_c2r(p, uh, u, DIM, st));
+    if (curl) {
+      const int nc = DIM == 3 ? 3 : 1;
+      SLES_TRY(launch(k_curl_hat<Tp, DIM>, 1184, 256, 0, st, (const C*)uh, slot(p, 0), p.hc_elems, N, p.nkp, p.nk));
+      SLES_TRY(TR::c2r(p, slot(p, 0), (Tp*)curl, nc, slot(p, 0), st));
+    }
+    return SLES_OK;
+  }
+  int velocity_gradient(PlanInfo& p, const void* uh, void* grad, cudaStream_t st) override {
+    for (int i = 0; i < DIM; ++i) {
+      SLES_TRY(launch(k_deriv_hat<Tp, DIM>, 1184, 256, 0, st, (const C*)uh, slot(p, 0), p.hc_elems, N, p.nkp, p.nk, i));
+      SLES_TRY(TR::c2r(p, slot(p, 0), (Tp*)grad + (long long)i * DIM * p.real_elems, DIM, slot(p, 0), st));
+    }
+    return SLES_OK;
+  }
+
+  // ---------------- fused passes ----------------
+  XArgs<Tp> xbase(const PlanInfo& p) const {
+    XArgs<Tp> a{};
+    a.ws = slot(p, 0);
+    a.fs = p.hc_elems;
+    a.nkp = p.nkp;
+    a.nk = p.nk;
+    a.nchunks = nchunks(p);
+    a.nu = (Tp)p.d.nu;
+    a.forcing = (Tp)p.d.forcing;
+    a.kmax = 2.0 / 3.0 * (double)(N / 2 + 1);  // initialize_domain.py:79
+    a.nu_d = p.d.nu;
+    return a;
+  }
+
+  template <int LES, int PAR2D>
+  int xpass(const PlanInfo& p, const XArgs<Tp>& a, cudaStream_t st) {
+    using K = XGeo<Tp, N, FX, W, GX>;
+    const long long items = (long long)(DIM == 3 ? N : 1) * nchunks(p);
+    return launch(k_xpass<Tp, N, FX, W, GX, DIM, LES, PAR2D>, (items + GX - 1) / GX, K::THREADS, K::SMEM, st, a);
+  }
+  int xpass_rt(const PlanInfo& p, const XArgs<Tp>& a, int les, int par2d, cudaStream_t st) {
+    if (!les) return xpass<0, 0>(p, a, st);
+    if (DIM == 2 && par2d) return xpass<1, 1>(p, a, st);
+    return xpass<1, 0>(p, a, st);
+  }
+
+  template <int LES>
+  int ypass(const PlanInfo& p, int inv, cudaStream_t st) {
+    if (DIM != 3) return SLES_OK;
+    using K = XGeo<Tp, N, FY, W, GY>;
+    YArgs<Tp> a{slot(p, 0), p.hc_elems, p.nkp, p.nk, nchunks(p)};
+    const long long items = (long long)N * nchunks(p);
+    if (inv) return launch(k_ypass_inv<Tp, N, FY, W, GY, LES>, (items + GY - 1) / GY, K::THREADS, K::SMEM, st, a);
+    return launch(k_ypass_fwd<Tp, N, FY, W, GY, LES>, (items + GY - 1) / GY, K::THREADS, K::SMEM, st, a);
+  }
+
+  template <int LES, int MODEL, int PAR2D>
+  int zpass(const PlanInfo& p, const Tp* uphys, const Tp* cphys, int stress_only, cudaStream_t st) {
+    using K = ZGeo<Tp, N, DIM, LES, PAR2D, LPI>;
+    ZArgs<Tp> a{};
+    a.ws = slot(p, 0);
+    a.fs = p.hc_elems;
+    a.nkp = p.nkp;
+    a.nlines = (DIM == 3) ? (long long)N * N : N;
+    a.scale = (Tp)(1.0 / (DIM == 3 ? (double)N * N * N : (double)N * N));
+    const double dx = 2.0 * 3.141592653589793 / N;  // initialize_domain.py:42
+    if (MODEL == M_SMAG) a.cdx2 = (Tp)((p.d.cs * dx) * (p.d.cs * dx));
+    else a.cdx2 = (Tp)(2.5 * p.d.cs * p.d.cs * dx * dx);
+    a.uphys = uphys;
+    a.cphys = cphys;
+    a.rs = p.real_elems;
+    a.stress_only = stress_only;
+    return launch(k_zpass<Tp, N, DIM, LES, MODEL, PAR2D, LPI>, (a.nlines + LPI - 1) / LPI, K::THREADS, K::SMEM, st, a);
+  }
+  int zpass_rt(const PlanInfo& p, int les, int model, int par2d, const Tp* uphys, const Tp* cphys, int so,
+               cudaStream_t st) {
+    if (!les) return zpass<0, M_NONE, 0>(p, uphys, cphys, so, st);
+    const int pz = (DIM == 2) ? par2d : 0;
+    if (model == SLES_LES_SMAGORINSKY) {
+      return pz ? zpass<1, M_SMAG, 1>(p, uphys, cphys, so, st) : zpass<1, M_SMAG, 0>(p, uphys, cphys, so, st);
+    }
+    return pz ? zpass<1, M_VREMAN, 1>(p, uphys, cphys, so, st) : zpass<1, M_VREMAN, 0>(p, uphys, cphys, so, st);
+  }
+
+  // One RHS evaluation ending in the X pass described by `fin`.
+  int pipeline(const PlanInfo& p, int les, const C* ucur, bool primed, const Tp* uphys, const Tp* cphys,
+               int stress_only, XArgs<Tp> fin, cudaStream_t st) {
+    const int model = p.d.les_model, par2d = p.d.parity;
+    if (!primed) {
+      XArgs<Tp> a0 = xbase(p);
+      a0.fwd = 0;
+      a0.prep = 1;
+      a0.uinv = ucur;
+      SLES_TRY(xpass_rt(p, a0, les, par2d, st));
+    }
+    SLES_TRY(les ? ypass<1>(p, 1, st) : ypass<0>(p, 1, st));
+    SLES_TRY(zpass_rt(p, les, model, par2d, uphys, cphys, stress_only, st));
+    SLES_TRY(les ? ypass<1>(p, 0, st) : ypass<0>(p, 0, st));
+    fin.fwd = 1;
+    return xpass_rt(p, fin, les, par2d, st);
+  }
+
+  // LES stress alone (masked, unprojected) into `out`: the T_hat the
+  // reference adds after recording F1 (RK4_method.py:65-70).
+  int stress_raw(const PlanInfo& p, const C* ucur, C* out, cudaStream_t st) {
+    XArgs<Tp> a = xbase(p);
+    a.kind = KX_RAW;
+    a.prep = 0;
+    a.ucur = ucur;
+    a.uout = out;
+    return pipeline(p, 1, ucur, false, nullptr, nullptr, 1, a, st);
+  }
+
+  int rhs(PlanInfo& p, const void* uh, const void* uphys, const void* cphys, void* du, void* f1,
+          cudaStream_t st) override {
+    const int les = p.d.les_model != SLES_LES_NONE;
+    XArgs<Tp> a = xbase(p);
+    a.kind = KX_RHS;
+    a.prep = 0;
+    a.ucur = (const C*)uh;
+    a.uout = (C*)du;
+    a.aux = (C*)f1;
+    if (f1) {
+      a.record_f1 = 1;
+      if (les && p.d.parity) {  // F1 = P(mask N + T) - T  (the reference records F1 before adding T back)
+        SLES_TRY(stress_raw(p, (const C*)uh, (C*)f1, st));
+        a.record_f1 = 2;
+      }
+    }
+    return pipeline(p, les, (const C*)uh, false, (const Tp*)uphys, (const Tp*)cphys, 0, a, st);
+  }
+
+  int stage(PlanInfo& p, int s, double dt, const void* ucur, const void* u0, void* u1, void* uout, void* aux,
+            const void* uphys, const void* cphys, int flags, cudaStream_t st) override {
+    const auto& d = p.d;
+    int les = d.les_model != SLES_LES_NONE;
+    XArgs<Tp> a = xbase(p);
+    a.ucur = (const C*)ucur;
+    a.u0 = (const C*)u0;
+    a.u1 = (C*)u1;
+    a.uout = (C*)uout;
+    a.aux = (C*)aux;
+    a.stage = s;
+    a.prep = (flags & STAGE_NO_PREPARE) ? 0 : 1;
+    bool primed = (flags & STAGE_PRIMED) != 0;
+    const int scheme = (flags & STAGE_RK4) ? SLES_RK4 : d.scheme;
+    static const double rk4a[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};  // initialize_domain.py:166
+    static const double rk4b[3] = {0.5, 0.5, 1.0};                              // initialize_domain.py:167
+    switch (scheme) {
+      case SLES_RK4:
+        if (s < 0 || s > 3) return SLES_ERR_INVALID_ARG;
+        a.kind = KX_RK4;
+        a.c1 = (Tp)(rk4a[s] * dt);
+        a.c2 = (Tp)(s < 3 ? rk4b[s] * dt : 0.0);
+        break;
+      case SLES_RK3:
+        if (s < 0 || s > 2) return SLES_ERR_INVALID_ARG;
+        if (d.parity) {
+          a.kind = KX_RK3P;
+          if (s == 0) a.c2 = (Tp)(0.5 * dt);
+          if (s == 1) { a.c1 = (Tp)dt; a.c2 = (Tp)(2.0 * dt); }
+          if (s == 2) a.c1 = (Tp)dt;
+        } else {
+          a.kind = KX_SSP3;
+          a.c1 = (Tp)dt;
+        }
+        break;
+      case SLES_ETD2:
+        if (s != 0 || !aux || !u1) return SLES_ERR_INVALID_ARG;
+        a.kind = d.parity ? KX_ETD2P : KX_ETD2C;
+        a.dt_d = dt;
+        if (d.parity && les) {  // ETD2_method.py:39-46 evaluates u x omega only
+          les = 0;
+          primed = false;  // the slots hold the LES pipeline's transforms
+        }
+        break;
+      default:
+        return SLES_ERR_INVALID_ARG;
+    }
+    if (flags & STAGE_RECORD_F1) {
+      if (!aux) return SLES_ERR_INVALID_ARG;
+      a.record_f1 = 1;
+      if (les && d.parity) {
+        SLES_TRY(stress_raw(p, (const C*)ucur, (C*)aux, st));
+        a.record_f1 = 2;
+        primed = false;
+      }
+    }
+    return pipeline(p, les, (const C*)ucur, primed, (const Tp*)uphys, (const Tp*)cphys, 0, a, st);
+  }
+
+  int diag(PlanInfo& p, const void* uh, const void* uphys, double* out, double* spec, int nshell,
+           cudaStream_t st) override {
+    if (nshell > max_shell(DIM, N)) nshell = max_shell(DIM, N);
+    if (!spec) nshell = 0;
+    double* part = reinterpret_cast<double*>(reinterpret_cast<char*>(p.ws) + WS_HEADER);
+    double* mpart = part + (size_t)DIAG_BLOCKS * (2 + max_shell(DIM, N));
+    const size_t smem = (nshell + 2 * DIAG_THREADS) * sizeof(double);
+    SLES_TRY(launch(k_diag_partial<Tp, DIM>, DIAG_BLOCKS, DIAG_THREADS, smem, st, (const C*)uh, p.hc_elems, N,
+                    p.nkp, p.nk, part, nshell));
+    int mblk = 0;
+    if (uphys) {
+      mblk = DIAG_BLOCKS;
+      SLES_TRY(launch(k_max_partial<Tp>, DIAG_BLOCKS, DIAG_THREADS, 0, st, (const Tp*)uphys,
+                      (long long)DIM * p.real_elems, mpart));
+    }
+    const double nd = (DIM == 3) ? (double)N * N * N : (double)N * N;
+    return launch(k_diag_final, 1, 256, 0, st, (const double*)part, DIAG_BLOCKS, nshell, (const double*)mpart, mblk,
+                  1.0 / (nd * nd), p.d.nu, out, spec);
+  }
+};
+
+// factories, defined in sles_n<N>.cu
+Engine* make_engine(int dtype, int dim, int n);
+
+}  // namespace sles
+
+#define SLES_DEFINE_ENGINES(NN)                                                   \
+  namespace sles {                                                               \
+  Engine* make_engine_##NN(int dtype, int dim) {                                 \
+    if (dtype == SLES_F32 && dim == 3) return new EngineImpl<float, NN, 3>();    \
+    if (dtype == SLES_F64 && dim == 3) return new EngineImpl<double, NN, 3>();   \
+    if (dtype == SLES_F32 && dim == 2) return new EngineImpl<float, NN, 2>();    \
+    if (dtype == SLES_F64 && dim == 2) return new EngineImpl<double, NN, 2>();   \
+    return nullptr;                                                              \
+  }                                                                              \
+  }

@@ -1,0 +1,321 @@
+// Register-resident Stockham line FFT for sm_100a.
+//
+// A line of L complex points is owned by T cooperating threads; thread j holds
+// the V = L/T points x[j + T*m] ("cyclic" distribution) in registers.  The
+// transform runs as up to three Stockham radix stages R0, R1, R2
+// (L = R0*R1*R2).  Every stage reads the cyclic distribution and performs
+// L/(R*T) radix-R butterflies per thread in registers (twiddle first, then the
+// DFT_R, Stockham autosort indexing idxD = (b/Ns)*Ns*R + b%Ns).  Between
+// stages the values are exchanged through a padded shared-memory line (one
+// pad slot every 16 points keeps the strided writes of the autosort free of
+// bank conflicts); the last stage writes its outputs straight back into the
+// cyclic registers, so input and output of a transform share the same
+// distribution and forward/inverse transforms and pointwise products chain in
+// registers without any shared-memory traffic.
+//
+// Stage twiddles are generated once per thread in float64 (sincospi) and
+// rounded once to the working precision.  Forward = exp(-2 pi i nk/L),
+// inverse = exp(+2 pi i nk/L), both unscaled.
+#pragma once
+#include "sles_common.cuh"
+
+namespace sles {
+
+// ---------------------------------------------------------------------------
+// small DFTs on registers, natural order in and out; DIR = -1 forward, +1 inverse
+// ---------------------------------------------------------------------------
+template <typename C, typename Tp>
+__device__ __forceinline__ C rot(C a, Tp c, Tp s) {  // a * (c + i s)
+  return cmk<C>(a.x * c - a.y * s, a.x * s + a.y * c);
+}
+
+template <int DIR, typename C>
+__device__ __forceinline__ void dft2(C& a, C& b) {
+  C t = a;
+  a = cadd(t, b);
+  b = csub(t, b);
+}
+
+template <int DIR, typename C>
+__device__ __forceinline__ void dft4(C& a0, C& a1, C& a2, C& a3) {
+  C t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = csub(a1, a3);
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  if (DIR < 0) {
+    a1 = cadd(t1, cmulmi(t3));
+    a3 = cadd(t1, cmuli(t3));
+  } else {
+    a1 = cadd(t1, cmuli(t3));
+    a3 = cadd(t1, cmulmi(t3));
+  }
+}
+
+template <int DIR, typename C>
+__device__ __forceinline__ void dft3(C& a0, C& a1, C& a2) {
+  using Tp = decltype(C::x);
+  const Tp h = (Tp)0.86602540378443864676;  // sin(2 pi / 3)
+  C s = cadd(a1, a2), d = csub(a1, a2);
+  C m = cmk<C>(a0.x - (Tp)0.5 * s.x, a0.y - (Tp)0.5 * s.y);
+  a0 = cadd(a0, s);
+  C id = cmk<C>(-d.y * h, d.x * h);  // i h d
+  if (DIR < 0) {
+    a1 = csub(m, id);
+    a2 = cadd(m, id);
+  } else {
+    a1 = cadd(m, id);
+    a2 = csub(m, id);
+  }
+}
+
+template <int R, int DIR, typename C>
+__device__ __forceinline__ void dft(C (&u)[R]) {
+  using Tp = decltype(C::x);
+  if constexpr (R == 1) {
+  } else if constexpr (R == 2) {
+    dft2<DIR>(u[0], u[1]);
+  } else if constexpr (R == 3) {
+    dft3<DIR>(u[0], u[1], u[2]);
+  } else if constexpr (R == 4) {
+    dft4<DIR>(u[0], u[1], u[2], u[3]);
+  } else if constexpr (R == 6) {
+    // 6 = 2 (inner, stride 3) x 3 (outer); X[k1 + 2 k2]
+    C y[3][2];
+#pragma unroll
+    for (int n2 = 0; n2 < 3; ++n2) {
+      y[n2][0] = u[n2];
+      y[n2][1] = u[n2 + 3];
+      dft2<DIR>(y[n2][0], y[n2][1]);
+    }
+    const Tp c = (Tp)0.5, s = (Tp)0.86602540378443864676;  // w6^1
+    y[1][1] = rot(y[1][1], c, (Tp)DIR * s);
+    y[2][1] = rot(y[2][1], -c, (Tp)DIR * s);  // w6^2
+#pragma unroll
+    for (int k1 = 0; k1 < 2; ++k1) {
+      dft3<DIR>(y[0][k1], y[1][k1], y[2][k1]);
+      u[k1] = y[0][k1];
+      u[k1 + 2] = y[1][k1];
+      u[k1 + 4] = y[2][k1];
+    }
+  } else if constexpr (R == 8) {
+    C e0 = u[0], e1 = u[2], e2 = u[4], e3 = u[6];
+    C o0 = u[1], o1 = u[3], o2 = u[5], o3 = u[7];
+    dft4<DIR>(e0, e1, e2, e3);
+    dft4<DIR>(o0, o1, o2, o3);
+    const Tp r = (Tp)0.70710678118654752440;
+    o1 = rot(o1, r, (Tp)DIR * r);
+    o2 = (DIR < 0) ? cmulmi(o2) : cmuli(o2);
+    o3 = rot(o3, -r, (Tp)DIR * r);
+    u[0] = cadd(e0, o0); u[4] = csub(e0, o0);
+    u[1] = cadd(e1, o1); u[5] = csub(e1, o1);
+    u[2] = cadd(e2, o2); u[6] = csub(e2, o2);
+    u[3] = cadd(e3, o3); u[7] = csub(e3, o3);
+  } else if constexpr (R == 16) {
+    // 16 = 4 (inner over n1, stride 4) x 4 (outer over n2); X[k1 + 4 k2]
+    C y[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+      y[n2][0] = u[n2];
+      y[n2][1] = u[n2 + 4];
+      y[n2][2] = u[n2 + 8];
+      y[n2][3] = u[n2 + 12];
+      dft4<DIR>(y[n2][0], y[n2][1], y[n2][2], y[n2][3]);
+    }
+    const Tp c1 = (Tp)0.92387953251128675613, s1 = (Tp)0.38268343236508977173;
+    const Tp r = (Tp)0.70710678118654752440;
+    const Tp d = (Tp)DIR;
+    y[1][1] = rot(y[1][1], c1, d * s1);   // w^1
+    y[1][2] = rot(y[1][2], r, d * r);     // w^2
+    y[1][3] = rot(y[1][3], s1, d * c1);   // w^3
+    y[2][1] = rot(y[2][1], r, d * r);     // w^2
+    y[2][2] = (DIR < 0) ? cmulmi(y[2][2]) : cmuli(y[2][2]);  // w^4
+    y[2][3] = rot(y[2][3], -r, d * r);    // w^6
+    y[3][1] = rot(y[3][1], s1, d * c1);   // w^3
+    y[3][2] = rot(y[3][2], -r, d * r);    // w^6
+    y[3][3] = rot(y[3][3], -c1, -d * s1); // w^9
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      dft4<DIR>(y[0][k1], y[1][k1], y[2][k1], y[3][k1]);
+      u[k1] = y[0][k1];
+      u[k1 + 4] = y[1][k1];
+      u[k1 + 8] = y[2][k1];
+      u[k1 + 12] = y[3][k1];
+    }
+  } else {
+    static_assert(R == 0, "unsupported radix");
+  }
+}
+
+// padded position in an exchange line: one pad slot after every 16 points
+__device__ __forceinline__ int xpad(int p) { return p + (p >> 4); }
+__host__ __device__ constexpr int xline_len(int L) { return L + L / 16 + 1; }
+
+// ---------------------------------------------------------------------------
+// Stockham line engine
+// ---------------------------------------------------------------------------
+template <typename Tp, int L_, int R0, int R1, int R2, int T_>
+struct LineFFT {
+  using C = typename CT<Tp>::C;
+  static constexpr int L = L_;
+  static constexpr int T = T_;
+  static constexpr int V = L / T;
+  static constexpr int S = (R1 == 1) ? 1 : ((R2 == 1) ? 2 : 3);
+  static_assert(R0 * R1 * R2 == L, "radix plan does not multiply to L");
+  static_assert((L / R0) % T == 0 && (L / R1) % T == 0 && (L / R2) % T == 0,
+                "threads per line must divide the butterfly count of every stage");
+  static constexpr int NB1 = (S >= 2) ? (L / R1) / T : 0;
+  static constexpr int NB2 = (S >= 3) ? (L / R2) / T : 0;
+  static constexpr int TW1 = (S >= 2) ? NB1 * (R1 - 1) : 1;
+  static constexpr int TW2 = (S >= 3) ? NB2 * (R2 - 1) : 1;
+
+  C tw1[TW1];
+  C tw2[TW2];
+
+  // forward twiddles of stage s for thread j (float64, rounded once)
+  __device__ __forceinline__ void init(int j) {
+    if constexpr (S >= 2) {
+#pragma unroll
+      for (int q = 0; q < NB1; ++q) {
+        int k = (j + T * q) % R0;
+#pragma unroll
+        for (int r = 1; r < R1; ++r) tw1[q * (R1 - 1) + r - 1] = twiddle<Tp>((long long)k * r, R0 * R1, -1);
+      }
+    }
+    if constexpr (S >= 3) {
+#pragma unroll
+      for (int q = 0; q < NB2; ++q) {
+        int k = (j + T * q) % (R0 * R1);
+#pragma unroll
+        for (int r = 1; r < R2; ++r) tw2[q * (R2 - 1) + r - 1] = twiddle<Tp>((long long)k * r, L, -1);
+      }
+    }
+  }
+
+  template <int R, int DIR, bool LAST, bool TWID, int NTW>
+  __device__ __forceinline__ void stage(C (&v)[V], const C (&tw)[NTW], int Ns, int j, C* sm, int ws) {
+    constexpr int NB = (L / R) / T;
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+      C u[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) u[r] = v[q + r * NB];
+      if constexpr (TWID) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          C w = tw[q * (R - 1) + r - 1];
+          u[r] = (DIR < 0) ? cmul(u[r], w) : cmulc(u[r], w);
+        }
+      }
+      dft<R, DIR>(u);
+      if constexpr (LAST) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[q + r * NB] = u[r];
+      } else {
+        int b = j + T * q;
+        int k = b % Ns;
+        int idxD = (b / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) sm[xpad(idxD + r * Ns) * ws] = u[r];
+      }
+    }
+  }
+
+  __device__ __forceinline__ void exchange(C (&v)[V], int j, C* sm, int ws) {
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < V; ++m) v[m] = sm[xpad(j + T * m) * ws];
+  }
+
+  // In-place transform of the cyclic registers.  sm: this line's exchange
+  // scratch (xline_len(L) slots of stride ws).  All threads of the block must
+  // call this uniformly (it contains __syncthreads when S > 1).  Convention
+  // shared by every user of an exchange scratch: a barrier precedes each
+  // write phase, so back-to-back transforms on one scratch are safe.
+  template <int DIR>
+  __device__ __forceinline__ void run(C (&v)[V], int j, C* sm, int ws) {
+    if constexpr (S >= 2) __syncthreads();
+    stage<R0, DIR, S == 1, false>(v, tw1, 1, j, sm, ws);
+    if constexpr (S >= 2) {
+      exchange(v, j, sm, ws);
+      if constexpr (S >= 3) __syncthreads();
+      stage<R1, DIR, S == 2, true>(v, tw1, R0, j, sm, ws);
+    }
+    if constexpr (S >= 3) {
+      exchange(v, j, sm, ws);
+      stage<R2, DIR, true, true>(v, tw2, R0 * R1, j, sm, ws);
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// radix plans per line length (complex points).  T = threads per line.
+// ---------------------------------------------------------------------------
+template <typename Tp, int L> struct PlanFor;
+template <typename Tp> struct PlanFor<Tp, 4>    { using F = LineFFT<Tp, 4, 4, 1, 1, 1>; };
+template <typename Tp> struct PlanFor<Tp, 6>    { using F = LineFFT<Tp, 6, 6, 1, 1, 1>; };
+template <typename Tp> struct PlanFor<Tp, 8>    { using F = LineFFT<Tp, 8, 8, 1, 1, 1>; };
+template <typename Tp> struct PlanFor<Tp, 12>   { using F = LineFFT<Tp, 12, 4, 3, 1, 1>; };
+template <typename Tp> struct PlanFor<Tp, 16>   { using F = LineFFT<Tp, 16, 4, 4, 1, 4>; };
+template <typename Tp> struct PlanFor<Tp, 24>   { using F = LineFFT<Tp, 24, 2, 4, 3, 2>; };
+template <typename Tp> struct PlanFor<Tp, 32>   { using F = LineFFT<Tp, 32, 8, 4, 1, 4>; };
+template <typename Tp> struct PlanFor<Tp, 48>   { using F = LineFFT<Tp, 48, 4, 4, 3, 4>; };
+template <typename Tp> struct PlanFor<Tp, 64>   { using F = LineFFT<Tp, 64, 8, 8, 1, 8>; };
+template <typename Tp> struct PlanFor<Tp, 96>   { using F = LineFFT<Tp, 96, 4, 4, 6, 8>; };
+template <typename Tp> struct PlanFor<Tp, 128>  { using F = LineFFT<Tp, 128, 16, 8, 1, 8>; };
+template <typename Tp> struct PlanFor<Tp, 256>  { using F = LineFFT<Tp, 256, 16, 16, 1, 16>; };
+template <typename Tp> struct PlanFor<Tp, 512>  { using F = LineFFT<Tp, 512, 16, 16, 2, 32>; };
+template <typename Tp> struct PlanFor<Tp, 1024> { using F = LineFFT<Tp, 1024, 16, 16, 4, 64>; };
+
+// Plans with at most 8-12 points per thread, for passes that keep several
+// transformed lines live in registers at once (one more exchange per line).
+template <typename Tp, int L> struct PlanLo { using F = typename PlanFor<Tp, L>::F; };
+template <typename Tp> struct PlanLo<Tp, 128> { using F = LineFFT<Tp, 128, 8, 4, 4, 16>; };
+template <typename Tp> struct PlanLo<Tp, 256> { using F = LineFFT<Tp, 256, 8, 8, 4, 32>; };
+template <typename Tp> struct PlanLo<Tp, 512> { using F = LineFFT<Tp, 512, 8, 8, 8, 64>; };
+
+// ---------------------------------------------------------------------------
+// real <-> half-complex via a half-length complex FFT (N = 2L real points)
+// ---------------------------------------------------------------------------
+// c2r pre-processing.  X(k) returns the half-complex input bin k in [0, L].
+// The imaginary parts of bins 0 and L are discarded (pocketfft/numpy irfft
+// semantics).  Produces Z'[k] = (X_k + conj X_{L-k}) + i (X_k - conj X_{L-k}) W_N^{-k}
+// in the cyclic registers; the unscaled inverse L-point FFT of Z' then yields
+// z'[n] = N*(x[2n] + i x[2n+1]).  twN[k] = exp(-2 pi i k/N), k < L.
+template <class F, class Src>
+__device__ __forceinline__ void c2r_pre(typename F::C (&v)[F::V], int j, const typename F::C* twN, Src X) {
+  using C = typename F::C;
+#pragma unroll
+  for (int m = 0; m < F::V; ++m) {
+    int k = j + F::T * m;
+    C a = X(k), b = X(F::L - k);
+    if (k == 0) { a.y = 0; b.y = 0; }
+    C e = cadd(a, cconj(b));
+    C o = cmulc(csub(a, cconj(b)), twN[k]);
+    v[m] = cadd(e, cmuli(o));
+  }
+}
+
+// r2c post-processing.  v holds Z = FFT_L(z) with z[n] = x[2n] + i x[2n+1];
+// emits out(k, X_k) for k in [0, L] (bin L by thread j == 0).  Uses the line's
+// exchange scratch; all threads of the block must call it uniformly.
+template <class F, class Dst>
+__device__ __forceinline__ void r2c_post(typename F::C (&v)[F::V], int j, typename F::C* sm, int ws,
+                                         const typename F::C* twN, Dst out) {
+  using C = typename F::C;
+  using Tp = decltype(C::x);
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < F::V; ++m) sm[xpad(j + F::T * m) * ws] = v[m];
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < F::V; ++m) {
+    int k = j + F::T * m;
+    C z = v[m];
+    C zc = cconj(sm[xpad((F::L - k) % F::L) * ws]);
+    C s = cadd(z, zc), d = csub(z, zc);
+    C t = cmulmi(cmul(twN[k], d));
+    out(k, cmk<C>((Tp)0.5 * (s.x + t.x), (Tp)0.5 * (s.y + t.y)));
+    if (k == 0) out(F::L, cmk<C>(z.x - z.y, (Tp)0));
+  }
+}
+
+}  // namespace sles

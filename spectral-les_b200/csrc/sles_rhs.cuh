@@ -1,0 +1,729 @@
+// Fused right-hand side + stage update (2D and 3D).
+//
+// One RHS evaluation in 3D is four kernels, each a single HBM pass:
+//
+//   Y1  inverse y-FFT      (x, ky, kz) -> (x, y, kz); applies i*ky where a
+//                          y-derivative is needed
+//   Z   fused z pass       per (x, y) line: c2r of the velocity and derivative
+//                          lines, pointwise u x omega and the eddy-viscosity
+//                          stress (Smagorinsky or Vreman), r2c of the products
+//   Y2  forward y-FFT      adds the ky, kz parts of div(tau)
+//   X   fused x pass       forward x-FFT, kx part of div(tau), 2/3 mask,
+//                          projection, forcing, viscous term, the integrator's
+//                          stage update, then the inverse x-FFT (and i*kx) of
+//                          the new state, which primes the next evaluation
+//
+// In 2D the r2c axis is y (axis 1): X and Z(=y) passes only.
+// Physical fields never touch HBM.  Derivatives along an axis are applied
+// while that axis is still spectral, so the inverse passes carry 6 (LES) or
+// 5 (no LES) fields rather than the 12 the reference transforms.
+//
+// Workspace slots (half-complex fields, updated in place pass to pass):
+//  3D LES:   X -> [0..2] A_c = X^-1(u_c), [3..5] B_c = X^-1(i kx u_c)
+//            Y1 -> [0..2] a_c, [3..5] dx_c, [6..8] dy_c
+//            Z  -> [0..2] N_c = rfft(u x omega), [3..8] F_xx F_xy F_xz F_yy F_yz F_zz
+//                  (F_ij = rfft(nu_t S_ij))
+//            Y2 -> [0..2] G_c = N_c + 2i(ky F_cy + kz F_cz), [3..5] H_c = F_cx
+//  3D plain: X -> [0..2] A_c, [3] X^-1(-i kx w), [4] X^-1(i kx v)
+//            Y1 -> [0..2] a_c, [3] Oy, [4] Oz, [5] Ox (curl parts without kz)
+//            Z  -> [0..2] N_c;  Y2 -> [0..2] in place
+//  2D plain: X -> [0] A_u, [1] A_v, [2] X^-1(i kx v);  Z -> [0] rfft(v w), [1] rfft(-u w)
+//  2D LES:   X -> [0] A_u, [1] A_v, [2] X^-1(i kx u), [3] X^-1(i kx v)
+//            Z -> [0] N_0, [1] N_1, then F12, F22 (reference arithmetic) or
+//                 F11, F12, F22 (corrected stress)
+//
+// Reference: computeRHS, src/RK4_method.py:38-71; U_cross_omega / del_cross_U /
+// velocity_gradient / residue_stress, src/math_formula.py:5-146;
+// calculate_nuR, src/smagorinsky.py:24-47 and src/vreman.py:30-147.
+#pragma once
+#include "sles_passes.cuh"
+
+namespace sles {
+
+enum StageKind { KX_RHS = 0, KX_RK4 = 1, KX_RK3P = 2, KX_SSP3 = 3, KX_ETD2P = 4, KX_ETD2C = 5, KX_RAW = 6 };
+enum LesModel { M_NONE = 0, M_SMAG = 1, M_VREMAN = 2 };
+
+template <typename Tp>
+struct XArgs {
+  using C = typename CT<Tp>::C;
+  C* ws;                 // workspace slot 0
+  long long fs;          // elements per half-complex field
+  int nkp, nk, nchunks;
+  int fwd;               // 1: forward part (RHS from the slots), 0: inverse only from uinv
+  int prep;              // 1: inverse part (prime the slots for the next evaluation)
+  const C* uinv;         // inverse-only source
+  const C* ucur;         // state the RHS is evaluated at
+  const C* u0;
+  C* u1;
+  C* uout;
+  C* aux;                // ETD2: new F1; record_f1: recorded F1
+  int kind, stage;
+  int record_f1;         // 1: aux = projected term; 2: aux = projected term - aux
+  Tp nu, forcing;
+  double kmax;
+  Tp c1, c2;             // stage coefficients (host-computed in float64)
+  double nu_d, dt_d;     // ETD2 weights are evaluated in float64
+};
+
+// Per-position spectral combine and stage update for D velocity components.
+// S[c] holds R_c (nonlinear + stress term before masking) on entry and the
+// new state (or dU) on exit.  k[c]: integer wavenumbers; off: element offset.
+template <typename Tp, int D>
+__device__ __forceinline__ void combine_update(const XArgs<Tp>& A, typename CT<Tp>::C (&S)[D], const int (&k)[D],
+                                               long long off) {
+  using C = typename CT<Tp>::C;
+  const long long fs = A.fs;
+  int k2 = 0;
+  bool in = true;
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    k2 += k[c] * k[c];
+    in = in && fabs((double)k[c]) < A.kmax;  // initialize_domain.py:109-114
+  }
+  const double kk = (double)(k2 == 0 ? 1 : k2);  // K_over_K2, initialize_domain.py:163-165
+  C R[D], Uc[D];
+  C P = cmk<C>(0, 0);
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    R[c] = in ? S[c] : cmk<C>(0, 0);  // dU *= dealias (RK4_method.py:48)
+    P = cadd(P, cscale(R[c], (Tp)((double)k[c] / kk)));
+  }
+  if (A.kind == KX_RAW) {  // masked term only (the LES stress T_hat)
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      A.uout[c * fs + off] = R[c];
+      S[c] = R[c];
+    }
+    return;
+  }
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    R[c] = csub(R[c], cscale(P, (Tp)k[c]));  // RK4_method.py:52-57
+    Uc[c] = A.ucur[c * fs + off];
+  }
+  if (A.forcing > (Tp)0 && k2 != 0) {  // RK4_method.py:58-64
+#pragma unroll
+    for (int c = 0; c < D; ++c) R[c] = cadd(R[c], cscale(Uc[c], A.forcing));
+  }
+  if (A.record_f1) {  // RK4_method.py:65-66
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+      A.aux[c * fs + off] = (A.record_f1 == 2) ? csub(R[c], A.aux[c * fs + off]) : R[c];
+  }
+  if (A.kind == KX_ETD2P || A.kind == KX_ETD2C) {
+    // parity: src/ETD2_method.py:16-29; corrected: Cox & Matthews (2002) eq. 22
+    const double z = A.dt_d * A.nu_d * (double)k2;
+    const double E = exp(-A.dt_d * A.nu_d * (double)k2);
+    double w1, w0;
+    if (A.kind == KX_ETD2P) {
+      const double nk2 = A.nu_d * (double)k2;
+      const double den = (k2 == 0) ? 1.0 : A.dt_d * (nk2 * nk2);
+      w1 = ((1.0 - z) + 2.0 * z) / den;
+      w0 = (-E + 1.0 - z) / den;
+    } else if (fabs(z) < 1e-2) {
+      const double h = A.dt_d;
+      w1 = h * (1.5 - 2.0 * z / 3.0 + z * z / 4.0 - z * z * z / 15.0);
+      w0 = h * (-0.5 + z / 6.0 - z * z / 24.0 + z * z * z / 120.0);
+    } else {
+      const double h = A.dt_d;
+      w1 = h * ((1.0 - z) * E - 1.0 + 2.0 * z) / (z * z);
+      w0 = h * (-E + 1.0 - z) / (z * z);
+    }
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      const C F0 = A.u1[c * fs + off];
+      const C un = cadd(cscale(Uc[c], (Tp)E), cadd(cscale(R[c], (Tp)w1), cscale(F0, (Tp)w0)));
+      A.aux[c * fs + off] = R[c];
+      A.uout[c * fs + off] = un;
+      S[c] = un;
+    }
+    return;
+  }
+  const Tp nk2 = A.nu * (Tp)k2;  // (nu * K2) * U_hat, RK4_method.py:67-68
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    const C dU = csub(R[c], cscale(Uc[c], nk2));
+    const long long o = c * fs + off;
+    C un;
+    switch (A.kind) {
+      case KX_RK4:  // RK4_method.py:20-27
+        if (A.stage < 3) {
+          A.u1[o] = cadd(A.u1[o], cscale(dU, A.c1));
+          un = cadd(A.u0[o], cscale(dU, A.c2));
+        } else {
+          un = cadd(A.u1[o], cscale(dU, A.c1));
+          A.u1[o] = un;
+        }
+        break;
+      case KX_RK3P:  // RK3_method.py:26-33
+        if (A.stage == 0) {
+          un = cadd(A.u0[o], cscale(dU, A.c2));
+        } else if (A.stage == 1) {
+          un = cadd(csub(A.u0[o], cscale(dU, A.c1)), cscale(dU, A.c2));
+        } else {
+          const C t = cadd(cadd(cscale(dU, (Tp)(1.0 / 6.0)), cscale(dU, (Tp)(2.0 / 3.0))), cscale(dU, (Tp)(1.0 / 6.0)));
+          un = cadd(A.u0[o], cscale(t, A.c1));
+        }
+        break;
+      case KX_SSP3:  // Shu & Osher (1988)
+        if (A.stage == 0) {
+          un = cadd(A.u0[o], cscale(dU, A.c1));
+        } else if (A.stage == 1) {
+          un = cadd(cscale(A.u0[o], (Tp)0.75), cscale(cadd(Uc[c], cscale(dU, A.c1)), (Tp)0.25));
+        } else {
+          un = cadd(cscale(A.u0[o], (Tp)(1.0 / 3.0)), cscale(cadd(Uc[c], cscale(dU, A.c1)), (Tp)(2.0 / 3.0)));
+        }
+        break;
+      default:  // KX_RHS
+        un = dU;
+        break;
+    }
+    A.uout[o] = un;
+    S[c] = un;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// X pass.  Work item = (ky slice [3D], column chunk of W last-axis wavenumbers);
+// lines along x.  PAR2D selects the reference's 2D stress (1) or the corrected one.
+// ---------------------------------------------------------------------------
+template <typename Tp, int N, class F, int W, int G>
+struct XGeo {
+  static constexpr int T = F::T, V = F::V, THREADS = G * W * T, SCR = xline_len(N) * W;
+  static constexpr size_t SMEM = (size_t)G * SCR * sizeof(typename CT<Tp>::C);
+};
+
+template <typename Tp, int N, class F, int W, int G, int DIM, int LES, int PAR2D>
+__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS) k_xpass(const XArgs<Tp> A) {
+  using K = XGeo<Tp, N, F, W, G>;
+  using C = typename CT<Tp>::C;
+  constexpr int T = K::T, V = K::V, D = DIM;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* scr = reinterpret_cast<C*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int l = tid % W, j = (tid / W) % T, g = tid / (W * T);
+  F fft;
+  fft.init(j);
+  const long long it = (long long)blockIdx.x * G + g;
+  const int chunk = (int)(it % A.nchunks);
+  const int sl = (int)(it / A.nchunks);            // ky slice (3D); 0 in 2D
+  const int nsl = (DIM == 3) ? N : 1;
+  const int col = chunk * W + l;
+  const bool ok = sl < nsl && col < A.nk;
+  const long long base = (long long)(sl < nsl ? sl : 0) * A.nkp + col;
+  const long long ps = (DIM == 3) ? (long long)N * A.nkp : (long long)A.nkp;
+  const long long fs = A.fs;
+  C* sm = scr + g * K::SCR + l;
+  C* ws = A.ws;
+  auto ld = [&](const C* f, C (&v)[V]) {
+#pragma unroll
+    for (int m = 0; m < V; ++m) v[m] = ok ? f[base + (j + T * m) * ps] : cmk<C>(0, 0);
+  };
+  auto st = [&](int slot, const C (&v)[V]) {
+    if (ok) {
+#pragma unroll
+      for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
+    }
+  };
+  auto kx_at = [&](int m) { return kc2c(j + T * m, N); };
+  C S[D][V];
+  if (A.fwd) {
+    if (DIM == 3) {
+#pragma unroll
+      for (int c = 0; c < D; ++c) {
+        ld(ws + c * fs, S[c]);
+        fft.template run<-1>(S[c], j, sm, W);
+        if (LES) {  // + 2i kx F_cx
+          C h[V];
+          ld(ws + (3 + c) * fs, h);
+          fft.template run<-1>(h, j, sm, W);
+#pragma unroll
+          for (int m = 0; m < V; ++m) S[c][m] = cadd(S[c][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+        }
+      }
+    } else {
+      const Tp ky2 = (Tp)(2 * col);
+#pragma unroll
+      for (int c = 0; c < D; ++c) {
+        ld(ws + c * fs, S[c]);
+        fft.template run<-1>(S[c], j, sm, W);
+      }
+      if (LES) {
+        // reference (math_formula.py:128-146): T_0 = 2i(kx F12 + ky F22), T_1 = 0
+        // corrected: T_0 = 2i(kx F11 + ky F12), T_1 = 2i(kx F12 + ky F22)
+        C h[V];
+        ld(ws + 2 * fs, h);
+        fft.template run<-1>(h, j, sm, W);
+#pragma unroll
+        for (int m = 0; m < V; ++m) S[0][m] = cadd(S[0][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+        ld(ws + 3 * fs, h);
+        fft.template run<-1>(h, j, sm, W);
+#pragma unroll
+        for (int m = 0; m < V; ++m) {
+          S[0][m] = cadd(S[0][m], cmuli_s(h[m], ky2));
+          if (!PAR2D) S[1][m] = cadd(S[1][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+        }
+        if (!PAR2D) {
+          ld(ws + 4 * fs, h);
+          fft.template run<-1>(h, j, sm, W);
+#pragma unroll
+          for (int m = 0; m < V; ++m) S[1][m] = cadd(S[1][m], cmuli_s(h[m], ky2));
+        }
+      }
+    }
+    if (ok) {
+#pragma unroll
+      for (int m = 0; m < V; ++m) {
+        C s[D];
+        int k[D];
+#pragma unroll
+        for (int c = 0; c < D; ++c) s[c] = S[c][m];
+        k[0] = kx_at(m);
+        if (DIM == 3) { k[1] = kc2c(sl, N); k[D - 1] = col; }
+        else k[1] = col;
+        combine_update<Tp, D>(A, s, k, base + (j + T * m) * ps);
+#pragma unroll
+        for (int c = 0; c < D; ++c) S[c][m] = s[c];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < D; ++c) ld(A.uinv + c * fs, S[c]);
+  }
+  if (!A.prep) return;  // uniform across the block
+  if (LES) {
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      C b[V];
+#pragma unroll
+      for (int m = 0; m < V; ++m) b[m] = cmuli_s(S[c][m], (Tp)kx_at(m));
+      fft.template run<+1>(b, j, sm, W);
+      st(D + c, b);
+      fft.template run<+1>(S[c], j, sm, W);
+      st(c, S[c]);
+    }
+  } else if (DIM == 3) {
+    C q[V];
+#pragma unroll
+    for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[2][m], -(Tp)kx_at(m));  // -i kx w
+    fft.template run<+1>(q, j, sm, W);
+    st(3, q);
+#pragma unroll
+    for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[1][m], (Tp)kx_at(m));   //  i kx v
+    fft.template run<+1>(q, j, sm, W);
+    st(4, q);
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      fft.template run<+1>(S[c], j, sm, W);
+      st(c, S[c]);
+    }
+  } else {
+    C q[V];
+#pragma unroll
+    for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[1][m], (Tp)kx_at(m));   //  i kx v
+    fft.template run<+1>(q, j, sm, W);
+    st(2, q);
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      fft.template run<+1>(S[c], j, sm, W);
+      st(c, S[c]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Y passes (3D): work item = (x, kz chunk); lines along y (stride nkp)
+// ---------------------------------------------------------------------------
+template <typename Tp>
+struct YArgs {
+  using C = typename CT<Tp>::C;
+  C* ws;
+  long long fs;
+  int nkp, nk, nchunks;
+};
+
+template <typename Tp, int N, class F, int W, int G, int LES>
+__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS) k_ypass_inv(const YArgs<Tp> A) {
+  using K = XGeo<Tp, N, F, W, G>;
+  using C = typename CT<Tp>::C;
+  constexpr int T = K::T, V = K::V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* scr = reinterpret_cast<C*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int l = tid % W, j = (tid / W) % T, g = tid / (W * T);
+  F fft;
+  fft.init(j);
+  const long long it = (long long)blockIdx.x * G + g;
+  const int chunk = (int)(it % A.nchunks);
+  const int x = (int)(it / A.nchunks);
+  const int col = chunk * W + l;
+  const bool ok = x < N && col < A.nk;
+  const long long base = (long long)(x < N ? x : 0) * N * A.nkp + col;
+  const long long ps = A.nkp, fs = A.fs;
+  C* sm = scr + g * K::SCR + l;
+  C* ws = A.ws;
+  auto ld = [&](int slot, C (&v)[V]) {
+#pragma unroll
+    for (int m = 0; m < V; ++m) v[m] = ok ? ws[slot * fs + base + (j + T * m) * ps] : cmk<C>(0, 0);
+  };
+  auto st = [&](int slot, const C (&v)[V]) {
+    if (ok) {
+#pragma unroll
+      for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
+    }
+  };
+  auto iky = [&](const C (&v)[V], C (&w)[V]) {
+#pragma unroll
+    for (int m = 0; m < V; ++m) w[m] = cmuli_s(v[m], (Tp)kc2c(j + T * m, N));
+  };
+  C v[V], w[V];
+  if (LES) {
+#pragma unroll 1
+    for (int c = 0; c < 3; ++c) {
+      ld(c, v);
+      iky(v, w);
+      fft.template run<+1>(v, j, sm, W);
+      st(c, v);
+      fft.template run<+1>(w, j, sm, W);
+      st(6 + c, w);
+      ld(3 + c, v);
+      fft.template run<+1>(v, j, sm, W);
+      st(3 + c, v);
+    }
+  } else {
+    ld(2, v);  // A_w -> a_w and Ox = Y^-1(i ky A_w)
+    iky(v, w);
+    fft.template run<+1>(v, j, sm, W);
+    st(2, v);
+    fft.template run<+1>(w, j, sm, W);
+    st(5, w);
+    ld(0, v);  // A_u -> a_u and Oz = Y^-1(Q_z - i ky A_u)
+    ld(4, w);
+#pragma unroll
+    for (int m = 0; m < V; ++m) w[m] = csub(w[m], cmuli_s(v[m], (Tp)kc2c(j + T * m, N)));
+    fft.template run<+1>(v, j, sm, W);
+    st(0, v);
+    fft.template run<+1>(w, j, sm, W);
+    st(4, w);
+    ld(1, v);
+    fft.template run<+1>(v, j, sm, W);
+    st(1, v);
+    ld(3, v);
+    fft.template run<+1>(v, j, sm, W);
+    st(3, v);
+  }
+}
+
+template <typename Tp, int N, class F, int W, int G, int LES>
+__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS) k_ypass_fwd(const YArgs<Tp> A) {
+  using K = XGeo<Tp, N, F, W, G>;
+  using C = typename CT<Tp>::C;
+  constexpr int T = K::T, V = K::V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* scr = reinterpret_cast<C*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int l = tid % W, j = (tid / W) % T, g = tid / (W * T);
+  F fft;
+  fft.init(j);
+  const long long it = (long long)blockIdx.x * G + g;
+  const int chunk = (int)(it % A.nchunks);
+  const int x = (int)(it / A.nchunks);
+  const int col = chunk * W + l;
+  const bool ok = x < N && col < A.nk;
+  const long long base = (long long)(x < N ? x : 0) * N * A.nkp + col;
+  const long long ps = A.nkp, fs = A.fs;
+  C* sm = scr + g * K::SCR + l;
+  C* ws = A.ws;
+  auto ld = [&](int slot, C (&v)[V]) {
+#pragma unroll
+    for (int m = 0; m < V; ++m) v[m] = ok ? ws[slot * fs + base + (j + T * m) * ps] : cmk<C>(0, 0);
+  };
+  auto st = [&](int slot, const C (&v)[V]) {
+    if (ok) {
+#pragma unroll
+      for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
+    }
+  };
+  if (!LES) {
+    C v[V];
+#pragma unroll 1
+    for (int c = 0; c < 3; ++c) {
+      ld(c, v);
+      fft.template run<-1>(v, j, sm, W);
+      st(c, v);
+    }
+    return;
+  }
+  const Tp kz2 = (Tp)(2 * col);
+  auto ky2 = [&](int m) { return (Tp)(2 * kc2c(j + T * m, N)); };
+  C t[V], acc[V], acc2[V];
+  // G_x = N_x + 2i(ky F_xy + kz F_xz);  H_y = F_xy, H_z = F_xz, H_x = F_xx
+  ld(4, t);
+  fft.template run<-1>(t, j, sm, W);
+  st(4, t);
+#pragma unroll
+  for (int m = 0; m < V; ++m) acc[m] = cmuli_s(t[m], ky2(m));
+  ld(5, t);
+  fft.template run<-1>(t, j, sm, W);
+  st(5, t);
+#pragma unroll
+  for (int m = 0; m < V; ++m) acc[m] = cadd(acc[m], cmuli_s(t[m], kz2));
+  ld(0, t);
+  fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+  for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc[m]);
+  st(0, t);
+  ld(3, t);
+  fft.template run<-1>(t, j, sm, W);
+  st(3, t);
+  // G_y = N_y + 2i(ky F_yy + kz F_yz);  G_z = N_z + 2i(ky F_yz + kz F_zz)
+  ld(6, t);
+  fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+  for (int m = 0; m < V; ++m) acc[m] = cmuli_s(t[m], ky2(m));
+  ld(7, t);
+  fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+  for (int m = 0; m < V; ++m) {
+    acc[m] = cadd(acc[m], cmuli_s(t[m], kz2));
+    acc2[m] = cmuli_s(t[m], ky2(m));
+  }
+  ld(1, t);
+  fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+  for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc[m]);
+  st(1, t);
+  ld(8, t);
+  fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+  for (int m = 0; m < V; ++m) acc2[m] = cadd(acc2[m], cmuli_s(t[m], kz2));
+  ld(2, t);
+  fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+  for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc2[m]);
+  st(2, t);
+}
+
+// ---------------------------------------------------------------------------
+// Z pass (the r2c axis: z in 3D, y in 2D).  Per line: c2r of NG physical
+// fields, pointwise products, r2c of NOUT products.  Threads: NG field groups
+// x LPI lines x T threads per line.
+// ---------------------------------------------------------------------------
+template <typename Tp>
+struct ZArgs {
+  using C = typename CT<Tp>::C;
+  C* ws;
+  long long fs;
+  int nkp;
+  long long nlines;      // N^(DIM-1)
+  Tp scale;              // 1/N^DIM
+  Tp cdx2;               // (Cs dx)^2 (Smagorinsky) or 2.5 Cs^2 dx^2 (Vreman)
+  const Tp* uphys;       // optional stored velocity (DIM real fields)
+  const Tp* cphys;       // optional stored curl (3 real fields in 3D, 1 in 2D)
+  long long rs;          // elements per real field
+  int stress_only;       // 1: drop u x omega (evaluates the LES stress alone)
+};
+
+template <typename Tp, int N, int DIM, int LES, int PAR2D, int LPI>
+struct ZGeo {
+  using F = typename PlanFor<Tp, N / 2>::F;
+  static constexpr int L = N / 2, T = F::T, V = F::V;
+  static constexpr int NG = (DIM == 3) ? (LES ? 12 : 6) : (LES ? 6 : 3);
+  static constexpr int NOUT = (DIM == 3) ? (LES ? 9 : 3) : (LES ? (PAR2D ? 4 : 5) : 2);
+  static constexpr int THREADS = NG * LPI * T;
+  static constexpr int LS = ((xline_len(L) + 15) / 16) * 16 + 8;
+  static constexpr size_t SMEM =
+      ((size_t)L + (size_t)NG * LPI * LS) * sizeof(typename CT<Tp>::C) + (size_t)NG * LPI * N * sizeof(Tp);
+};
+
+template <typename Tp, int MODEL>
+__device__ __forceinline__ Tp eddy_viscosity_3d(Tp a11, Tp a12, Tp a13, Tp a21, Tp a22, Tp a23, Tp a31, Tp a32,
+                                                Tp a33, Tp cdx2) {
+  if (MODEL == M_SMAG) {  // smagorinsky.py:31-39
+    const Tp ss = a11 * a11 + ((Tp)0.5 * ((a12 + a21) * (a12 + a21))) + a22 * a22 +
+                  ((Tp)0.5 * ((a13 + a31) * (a13 + a31))) + ((Tp)0.5 * ((a23 + a32) * (a23 + a32))) + a33 * a33;
+    return sqrt((Tp)2 * ss) * cdx2;
+  }
+  // vreman.py:32-123: B_beta from b_pq = sum_m a_mp a_mq, gate on alpha:alpha
+  const Tp b11 = a11 * a11 + a21 * a21 + a31 * a31;
+  const Tp b22 = a12 * a12 + a22 * a22 + a32 * a32;
+  const Tp b33 = a13 * a13 + a23 * a23 + a33 * a33;
+  const Tp b12 = a11 * a12 + a21 * a22 + a31 * a32;
+  const Tp b13 = a11 * a13 + a21 * a23 + a31 * a33;
+  const Tp b23 = a12 * a13 + a22 * a23 + a32 * a33;
+  const Tp B = (b11 * b22) - (b12 * b12) + (b11 * b33) - (b13 * b13) + (b22 * b33) - (b23 * b23);
+  const Tp sb = sqrt(B);  // NaN for a round-off negative B, as in the reference
+  const Tp aa = a11 * a11 + a12 * a12 + a13 * a13 + a21 * a21 + a22 * a22 + a23 * a23 + a31 * a31 + a32 * a32 +
+                a33 * a33;
+  const Tp gate = ((aa > (Tp)10e-5) && (sb > aa / (Tp)10e6)) ? sqrt((Tp)1 / aa) : (Tp)0;
+  return sb * (gate * cdx2);
+}
+
+template <typename Tp, int MODEL>
+__device__ __forceinline__ Tp eddy_viscosity_2d(Tp a11, Tp a12, Tp a21, Tp a22, Tp cdx2) {
+  if (MODEL == M_SMAG) {  // smagorinsky.py:41-46
+    const Tp ss = (a11 * a11) + ((Tp)0.5 * ((a12 + a21) * (a12 + a21))) + (a22 * a22);
+    return sqrt((Tp)2 * ss) * cdx2;
+  }
+  // vreman.py:125-147
+  const Tp b11 = a11 * a11 + a21 * a21, b22 = a12 * a12 + a22 * a22, b12 = a11 * a12 + a21 * a22;
+  const Tp sb = sqrt((b11 * b22) - (b12 * b12));
+  const Tp aa = a11 * a11 + a12 * a12 + a21 * a21 + a22 * a22;
+  const Tp gate = ((aa > (Tp)10e-5) && (sb > aa / (Tp)10e6)) ? sqrt((Tp)1 / aa) : (Tp)0;
+  return sb * (gate * cdx2);
+}
+
+// Pointwise products on the stash (field stride ps, point p).  uo/co: the
+// stored physical velocity / curl at this point, or null.
+template <typename Tp, int DIM, int LES, int MODEL, int PAR2D>
+__device__ __forceinline__ void z_pointwise(Tp* st, int ps, int p, const Tp* uo, const Tp* co, Tp cdx2) {
+  auto S = [&](int f) -> Tp& { return st[f * ps + p]; };
+  if (DIM == 3) {
+    Tp u = S(0), v = S(1), w = S(2);
+    Tp ox, oy, oz;
+    Tp a11 = 0, a12 = 0, a13 = 0, a21 = 0, a22 = 0, a23 = 0, a31 = 0, a32 = 0, a33 = 0;
+    if (LES) {  // a[i][j] = d u_j / d x_i (math_formula.py:27-62)
+      a11 = S(3); a12 = S(4); a13 = S(5);
+      a21 = S(6); a22 = S(7); a23 = S(8);
+      a31 = S(9); a32 = S(10); a33 = S(11);
+      ox = a23 - a32; oy = a31 - a13; oz = a12 - a21;
+    } else {
+      ox = S(3); oy = S(4); oz = S(5);
+    }
+    if (uo) { u = uo[0]; v = uo[1]; w = uo[2]; }
+    if (co) { ox = co[0]; oy = co[1]; oz = co[2]; }
+    S(0) = v * oz - w * oy;  // math_formula.py:9-11
+    S(1) = w * ox - u * oz;
+    S(2) = u * oy - v * ox;
+    if (LES) {
+      const Tp nu = eddy_viscosity_3d<Tp, MODEL>(a11, a12, a13, a21, a22, a23, a31, a32, a33, cdx2);
+      S(3) = a11 * nu;  // math_formula.py:76-127
+      S(4) = ((Tp)0.5 * (a12 + a21)) * nu;
+      S(5) = ((Tp)0.5 * (a13 + a31)) * nu;
+      S(6) = a22 * nu;
+      S(7) = ((Tp)0.5 * (a23 + a32)) * nu;
+      S(8) = a33 * nu;
+    }
+  } else {
+    Tp u = S(0), v = S(1);
+    Tp om;
+    Tp a11 = 0, a12 = 0, a21 = 0, a22 = 0;
+    if (LES) {
+      a11 = S(2); a12 = S(3); a21 = S(4); a22 = S(5);
+      om = a12 - a21;
+    } else {
+      om = S(2);
+    }
+    if (uo) { u = uo[0]; v = uo[1]; }
+    if (co) om = co[0];
+    S(0) = v * om;  // math_formula.py:7-8
+    S(1) = -u * om;
+    if (LES) {
+      const Tp nu = eddy_viscosity_2d<Tp, MODEL>(a11, a12, a21, a22, cdx2);
+      const Tp f12 = ((Tp)0.5 * (a12 + a21)) * nu, f22 = a22 * nu;
+      if (PAR2D) { S(2) = f12; S(3) = f22; }
+      else { S(2) = a11 * nu; S(3) = f12; S(4) = f22; }
+    }
+  }
+}
+
+template <typename Tp, int N, int DIM, int LES, int MODEL, int PAR2D, int LPI>
+__global__ void __launch_bounds__(ZGeo<Tp, N, DIM, LES, PAR2D, LPI>::THREADS) k_zpass(const ZArgs<Tp> A) {
+  using K = ZGeo<Tp, N, DIM, LES, PAR2D, LPI>;
+  using F = typename K::F;
+  using C = typename CT<Tp>::C;
+  constexpr int T = K::T, V = K::V, L = K::L;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* twN = reinterpret_cast<C*>(smem_raw);
+  C* scr = twN + L;
+  Tp* stash = reinterpret_cast<Tp*>(scr + K::NG * LPI * K::LS);
+  constexpr int PS = LPI * N;  // stash field stride
+  fill_twN<Tp, N>(twN);
+  __syncthreads();
+  const int tid = threadIdx.x;
+  const int j = tid % T, ln = (tid / T) % LPI, grp = tid / (T * LPI);
+  F fft;
+  fft.init(j);
+  const long long line0 = (long long)blockIdx.x * LPI;
+  const long long line = line0 + ln;
+  const bool ok = line < A.nlines;
+  const long long lo = (ok ? line : 0) * A.nkp;
+  const long long fs = A.fs;
+  C* sm = scr + (grp * LPI + ln) * K::LS;
+  const C* ws = A.ws;
+  // ---- phase A: c2r of physical field `grp` = slot s1 + sgn * i k * slot s2
+  {
+    int s1 = grp, s2 = -1;
+    Tp sgn = 0;
+    if (DIM == 3) {
+      if (LES) {
+        if (grp >= 9) { s1 = -1; s2 = grp - 9; sgn = 1; }      // d/dz u_c = i kz a_c
+      } else {
+        if (grp == 3) { s1 = 5; s2 = 1; sgn = -1; }             // omega_x = Ox - i kz v
+        else if (grp == 4) { s1 = 3; s2 = 0; sgn = 1; }         // omega_y = Oy + i kz u
+        else if (grp == 5) { s1 = 4; }                          // omega_z = Oz
+      }
+    } else {
+      if (LES) {
+        if (grp == 4) { s1 = -1; s2 = 0; sgn = 1; }             // a21 = du/dy
+        else if (grp == 5) { s1 = -1; s2 = 1; sgn = 1; }        // a22 = dv/dy
+      } else if (grp == 2) {
+        s1 = 2; s2 = 0; sgn = -1;                               // omega = X^-1(i kx v) - i ky u
+      }
+    }
+    C v[V];
+    c2r_pre<F>(v, j, twN, [&](int k) {
+      C r = cmk<C>(0, 0);
+      if (!ok) return r;
+      if (s1 >= 0) r = ws[s1 * fs + lo + k];
+      if (s2 >= 0) r = cadd(r, cmuli_s(ws[s2 * fs + lo + k], sgn * (Tp)k));
+      return r;
+    });
+    fft.template run<+1>(v, j, sm, 1);
+    C* dst = reinterpret_cast<C*>(stash + grp * PS + ln * N);
+#pragma unroll
+    for (int m = 0; m < V; ++m) dst[j + T * m] = cscale(v[m], A.scale);
+  }
+  __syncthreads();
+  // ---- phase B: pointwise products
+  for (int p = tid; p < PS; p += K::THREADS) {
+    const long long pl = line0 + p / N;
+    if (pl >= A.nlines) continue;
+    const long long o = pl * N + (p % N);
+    Tp ub[3], cb[3];
+    const Tp* uo = nullptr;
+    const Tp* co = nullptr;
+    if (A.uphys) {
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) ub[c] = A.uphys[c * A.rs + o];
+      uo = ub;
+    }
+    if (A.cphys) {
+#pragma unroll
+      for (int c = 0; c < (DIM == 3 ? 3 : 1); ++c) cb[c] = A.cphys[c * A.rs + o];
+      co = cb;
+    }
+    z_pointwise<Tp, DIM, LES, MODEL, PAR2D>(stash, PS, p, uo, co, A.cdx2);
+    if (A.stress_only) {
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) stash[c * PS + p] = (Tp)0;
+    }
+  }
+  __syncthreads();
+  // ---- phase C: r2c of product `grp` (groups >= NOUT run idle for the barriers)
+  {
+    const int gi = grp < K::NOUT ? grp : 0;
+    C v[V];
+    const C* src = reinterpret_cast<const C*>(stash + gi * PS + ln * N);
+#pragma unroll
+    for (int m = 0; m < V; ++m) v[m] = src[j + T * m];
+    fft.template run<-1>(v, j, sm, 1);
+    C* out = A.ws + gi * fs + lo;
+    const bool wr = ok && grp < K::NOUT;
+    r2c_post<F>(v, j, sm, 1, twN, [&](int k, C x) {
+      if (wr) out[k] = x;
+    });
+  }
+}
+
+}  // namespace sles

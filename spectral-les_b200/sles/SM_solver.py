@@ -1,0 +1,89 @@
+"""Driver loop (src/SM_solver.py:18-83) with the reference's adaptive dt.
+
+The loop, its CFL rule (dt = min(CFL dx/u_max, 0.1 dx^2/nu), with CFL = 0.3 on
+the first step), the NaN stop and the "time per gridpoint per timestep" print
+follow the reference.  Energy-spectrum snapshots go to Ek_plot_data.csv with
+the reference's binning; the PNG plot and the HDF5 field dumps are not
+produced (plotting and parallel HDF5 are outside this library).
+"""
+from __future__ import annotations
+
+import os
+import time
+
+import numpy as np
+
+from . import ETD2_method as ETD2
+from . import RK3_method as RK3
+from . import RK4_method as RK4
+from .diagnostics import max_velocity, reference_binned_spectrum
+
+__all__ = ["spectralMethodSolver", "find_max_velocity", "compute_dt"]
+
+
+def find_max_velocity(U, comm=None):
+    """Signed max over all components and points (src/SM_solver.py:245-255)."""
+    import torch
+    if isinstance(U, torch.Tensor):
+        return float(torch.max(U).item())
+    return float(np.max(np.array([np.max(np.asarray(u)) for u in U])))
+
+
+def compute_dt(U, u_max, nu, comm=None, dx=1.0, CFL=0.5):
+    """src/SM_solver.py:258-277; raises SystemExit where the reference exits."""
+    dt1 = CFL * dx / u_max
+    dt2 = 0.1 * dx ** 2 / nu if (nu > 0) else 1e6
+    dt = min(dt1, dt2)
+    if dt < 1e-6:
+        print(f"\n\n ###  Time step (dt = {dt:g}) is smaller than 1e-6  ###\n\n")
+        raise SystemExit(1)
+    return dt
+
+
+def _step(domain):
+    if domain.method == "RK4":
+        RK4.solveForNextTimestep(domain)
+    elif domain.method == "ETD2":
+        ETD2.solveForNextTimestep(domain)
+    elif domain.method == "RK3":
+        RK3.solveForNextTimestep(domain)
+    else:
+        raise ValueError("Invalid method name")
+
+
+def spectralMethodSolver(domain, file_out_time: float = 0.0, No_Ek_plot: int = 5, verbose: bool = True):
+    d = domain
+    u_max = max_velocity(d)
+    d.dt = compute_dt(None, u_max, d.nu, dx=d.dx, CFL=0.3)
+    t = d.dt
+    Ek_interval = d.T / No_Ek_plot if No_Ek_plot != 0 else 0
+    Ek_counter = 0
+    start = time.time()
+    d.U_hat1[...] = d.U_hat            # src/SM_solver.py:33
+    columns = {}
+    counter = 0
+    while True:
+        if Ek_interval > 0 and t >= Ek_counter:
+            tk, tE = reference_binned_spectrum(d)
+            columns[f"k-{t:g}"] = tk
+            columns[f"Ek-{t:g}"] = tE
+            Ek_counter += Ek_interval
+        if (t >= d.T) or (d.dt < 1e-8):
+            break
+        t += d.dt
+        _step(d)
+        u_max = max_velocity(d)
+        d.dt = compute_dt(None, u_max, d.nu, dx=d.dx, CFL=d.CFL)
+        if d.dt != d.dt:
+            if verbose:
+                print("\n############ dt = Nan #############\n", counter)
+            break
+        counter += 1
+    if columns:
+        import pandas as pd
+        pd.DataFrame(columns).to_csv("Ek_plot_data.csv", index=False)
+    total = time.time() - start
+    if verbose and counter > 0:
+        print(f"=>  run time: {total} sec")
+        print(f"Time per gridpoint per timestep: {total * d.num_processes / (d.N ** d.dim * counter)}\n")
+    return counter

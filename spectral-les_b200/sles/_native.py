@@ -1,0 +1,165 @@
+"""ctypes binding of libsles_b200.so (the C ABI declared in include/sles.h).
+
+Only plain pointers, sizes and a CUDA stream handle cross the boundary; torch
+is used for device memory and streams.  There is no CPU fallback: loading
+fails loudly if the library is missing or no CUDA device is present.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import torch
+
+LIB_NAME = "libsles_b200.so"
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+
+SLES_F32, SLES_F64 = 0, 1
+LES_NONE, LES_SMAGORINSKY, LES_VREMAN = 0, 1, 2
+SCHEME_RK4, SCHEME_RK3, SCHEME_ETD2 = 0, 1, 2
+STAGE_RECORD_F1, STAGE_PRIMED, STAGE_NO_PREPARE, STAGE_RK4 = 1, 2, 4, 8
+
+EXPORTED = [
+    "sles_plan_create", "sles_plan_destroy", "sles_plan_layout", "sles_plan_workspace_bytes",
+    "sles_plan_set_workspace", "sles_plan_set_params", "sles_fft_r2c", "sles_fft_c2r",
+    "sles_velocity_curl", "sles_velocity_gradient", "sles_rhs", "sles_stage", "sles_diag",
+    "sles_status_string", "sles_version",
+]
+
+
+class PlanDesc(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("n", ctypes.c_int), ("dtype", ctypes.c_int),
+                ("les_model", ctypes.c_int), ("scheme", ctypes.c_int), ("parity", ctypes.c_int),
+                ("nu", ctypes.c_double), ("cs", ctypes.c_double), ("forcing", ctypes.c_double)]
+
+
+class Layout(ctypes.Structure):
+    _fields_ = [("hc_elems", ctypes.c_int64), ("real_elems", ctypes.c_int64),
+                ("nkp", ctypes.c_int32), ("nk", ctypes.c_int32)]
+
+
+class SlesError(RuntimeError):
+    def __init__(self, status, where):
+        self.status = status
+        msg = _lib.sles_status_string(status).decode() if _lib else str(status)
+        super().__init__("%s failed: %s (status %d)" % (where, msg, status))
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the shared library and declare every entry point's signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("%s is not built (run `make -C spectral-les_b200/csrc -j8` or "
+                           "`python -c 'import __graft_entry__ as g; g.build()'`)" % path)
+    L = ctypes.CDLL(path)
+    vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    sig = {
+        "sles_plan_create": (i, [ctypes.POINTER(PlanDesc), ctypes.POINTER(vp)]),
+        "sles_plan_destroy": (i, [vp]),
+        "sles_plan_layout": (i, [vp, ctypes.POINTER(Layout)]),
+        "sles_plan_workspace_bytes": (ctypes.c_size_t, [vp]),
+        "sles_plan_set_workspace": (i, [vp, vp, ctypes.c_size_t]),
+        "sles_plan_set_params": (i, [vp, d, d, d]),
+        "sles_fft_r2c": (i, [vp, vp, vp, i, vp]),
+        "sles_fft_c2r": (i, [vp, vp, vp, i, vp]),
+        "sles_velocity_curl": (i, [vp, vp, vp, vp, vp]),
+        "sles_velocity_gradient": (i, [vp, vp, vp, vp]),
+        "sles_rhs": (i, [vp, vp, vp, vp, vp, vp, vp]),
+        "sles_stage": (i, [vp, i, d, vp, vp, vp, vp, vp, vp, vp, i, vp]),
+        "sles_diag": (i, [vp, vp, vp, vp, vp, i, vp]),
+        "sles_status_string": (ctypes.c_char_p, [i]),
+        "sles_version": (i, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status, where):
+    if status != 0:
+        raise SlesError(status, where)
+
+
+def ptr(t):
+    """Device pointer of a tensor (None -> NULL)."""
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def stream_handle(device=None):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+class Plan:
+    """Owns a ``sles_plan`` and its workspace (from torch's caching allocator)."""
+
+    def __init__(self, dim, n, dtype, les_model, scheme, parity, nu, cs, forcing, device):
+        if not torch.cuda.is_available():
+            raise RuntimeError("the spectral-LES B200 path needs a CUDA device; there is no CPU fallback")
+        L = load_library()
+        self.L = L
+        self.device = torch.device(device)
+        self.desc = PlanDesc(dim, n, SLES_F64 if dtype == torch.float64 else SLES_F32, les_model, scheme,
+                             1 if parity else 0, float(nu), float(cs), float(forcing))
+        h = ctypes.c_void_p()
+        check(L.sles_plan_create(ctypes.byref(self.desc), ctypes.byref(h)), "sles_plan_create")
+        self.h = h
+        lay = Layout()
+        check(L.sles_plan_layout(h, ctypes.byref(lay)), "sles_plan_layout")
+        self.hc_elems, self.real_elems, self.nkp, self.nk = lay.hc_elems, lay.real_elems, lay.nkp, lay.nk
+        nbytes = int(L.sles_plan_workspace_bytes(h))
+        with torch.cuda.device(self.device):
+            self.workspace = torch.empty(nbytes + 256, dtype=torch.uint8, device=self.device)
+        off = (-self.workspace.data_ptr()) % 256
+        self._ws_ptr = self.workspace.data_ptr() + off
+        check(L.sles_plan_set_workspace(h, ctypes.c_void_p(self._ws_ptr), ctypes.c_size_t(nbytes)),
+              "sles_plan_set_workspace")
+
+    def set_params(self, nu, cs, forcing):
+        check(self.L.sles_plan_set_params(self.h, float(nu), float(cs), float(forcing)), "sles_plan_set_params")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.sles_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # thin wrappers; tensors must be contiguous padded storage of this plan
+    def fft_r2c(self, real, hc, nf):
+        check(self.L.sles_fft_r2c(self.h, ptr(real), ptr(hc), nf, stream_handle(self.device)), "sles_fft_r2c")
+
+    def fft_c2r(self, hc, real, nf):
+        check(self.L.sles_fft_c2r(self.h, ptr(hc), ptr(real), nf, stream_handle(self.device)), "sles_fft_c2r")
+
+    def velocity_curl(self, uh, u, curl):
+        check(self.L.sles_velocity_curl(self.h, ptr(uh), ptr(u), ptr(curl), stream_handle(self.device)),
+              "sles_velocity_curl")
+
+    def velocity_gradient(self, uh, grad):
+        check(self.L.sles_velocity_gradient(self.h, ptr(uh), ptr(grad), stream_handle(self.device)),
+              "sles_velocity_gradient")
+
+    def rhs(self, uh, du, f1=None, uphys=None, cphys=None):
+        check(self.L.sles_rhs(self.h, ptr(uh), ptr(uphys), ptr(cphys), ptr(du), ptr(f1),
+                              stream_handle(self.device)), "sles_rhs")
+
+    def stage(self, stage, dt, ucur, u0, u1, uout, aux=None, uphys=None, cphys=None, flags=0):
+        check(self.L.sles_stage(self.h, int(stage), float(dt), ptr(ucur), ptr(u0), ptr(u1), ptr(uout), ptr(aux),
+                                ptr(uphys), ptr(cphys), int(flags), stream_handle(self.device)), "sles_stage")
+
+    def diag(self, uh, out, uphys=None, spectrum=None):
+        ns = 0 if spectrum is None else spectrum.numel()
+        check(self.L.sles_diag(self.h, ptr(uh), ptr(uphys), ptr(out), ptr(spectrum), ns,
+                               stream_handle(self.device)), "sles_diag")
