@@ -126,12 +126,23 @@ int sles_rhs(sles_plan* plan, const void* u_hat, const void* u_phys, const void*
  *   u_cur   : U_hat the RHS is evaluated at (read)
  *   u0      : U_hat at the start of the step (read; RK stages)
  *   u1      : RK4 accumulator U_hat1 (read+write); ETD2: F1 of the previous step (read)
- *   u_out   : new U_hat (write; may alias u_cur)
- *   aux_out : RK4 last stage: second copy of the result; ETD2: new F1 (write)
+ *   u_out   : new U_hat (write; may alias u_cur).  RK4 stage 3 writes the
+ *             result to both u1 and u_out (U_hat = U_hat1, src/RK4_method.py:27)
+ *   aux_out : ETD2: new F1 (write); with SLES_STAGE_RECORD_F1: recorded F1
  * stage: RK4 0..3, RK3 0..2, ETD2 0.  dt: step size.  u_phys / curl_phys as in
- * sles_rhs.  flags: SLES_STAGE_* below.
+ * sles_rhs.  flags (bitwise OR):
+ *   SLES_STAGE_RECORD_F1  record the reference's ETD2 F1 in aux_out
+ *   SLES_STAGE_PRIMED     the workspace already holds the x-inverse transforms
+ *                         of u_cur (written by the previous stage's call)
+ *   SLES_STAGE_NO_PREPARE skip the inverse transforms of u_out that prime the
+ *                         next stage
+ *   SLES_STAGE_RK4        run an RK4 stage whatever the plan's scheme (ETD2's
+ *                         first step, src/ETD2_method.py:8-14)
+ * Stage updates use the reference's expressions (RK3: U0 + (dt/2) dU,
+ * U0 - dt dU + (2 dt) dU, U0 + dt (dU/6 + 2 dU/3 + dU/6)); with parity = 0 the
+ * RK3 plan runs SSP-RK3 and ETD2 the Cox-Matthews weights.
  */
-enum { SLES_STAGE_RECORD_F1 = 1 };
+enum { SLES_STAGE_RECORD_F1 = 1, SLES_STAGE_PRIMED = 2, SLES_STAGE_NO_PREPARE = 4, SLES_STAGE_RK4 = 8 };
 int sles_stage(sles_plan* plan, int stage, double dt, const void* u_cur, const void* u0, void* u1,
                void* u_out, void* aux_out, const void* u_phys, const void* curl_phys, int flags,
                void* stream);
@@ -145,6 +156,16 @@ int sles_stage(sles_plan* plan, int stage, double dt, const void* u_cur, const v
  */
 int sles_diag(sles_plan* plan, const void* u_hat, const void* u_phys, double* out, double* spectrum,
               int nshell, void* stream);
+
+/*
+ * Profiling helper (no counterpart in the reference): runs the kernels of one
+ * fused RHS evaluation at u_hat ``iters`` times, timing each kernel class with
+ * CUDA events on ``stream``, and writes the mean milliseconds per launch to
+ * ms[0..4] = {x-inverse (priming), y-inverse, z, y-forward, x-forward+combine}
+ * (2D: y entries are 0).  du_scratch receives dU.  Synchronizes the stream.
+ */
+int sles_profile_rhs(sles_plan* plan, const void* u_hat, void* du_scratch, int iters, double* ms,
+                     void* stream);
 
 /* Human-readable text for a status code (static storage). */
 const char* sles_status_string(int status);

@@ -179,4 +179,10 @@ int sles_diag(sles_plan* p, const void* uh, const void* uphys, double* out, doub
   return p->eng->diag(p->info, uh, uphys, out, spectrum, nshell, (cudaStream_t)stream);
 }
 
+int sles_profile_rhs(sles_plan* p, const void* uh, void* du, int iters, double* ms, void* stream) {
+  if (int s = ready(p)) return s;
+  if (!uh || !du || !ms || iters < 1) return SLES_ERR_INVALID_ARG;
+  return p->eng->profile_rhs(p->info, uh, du, iters, ms, (cudaStream_t)stream);
+}
+
 }  // extern "C"

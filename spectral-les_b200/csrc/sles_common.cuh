@@ -48,6 +48,54 @@ __device__ __forceinline__ void raise_flag(unsigned* flag, unsigned bit) {
   if (flag) atomicOr(flag, bit);
 }
 
+// ---------------------------------------------------------------------------
+// TMA bulk copies (global -> shared) completed on an mbarrier.  Every wait is
+// bounded: after MBAR_SPIN_LIMIT polls the wait raises SLES_ERRF_WAIT_TIMEOUT
+// in the error word and returns false, so a kernel never spins forever.
+// ---------------------------------------------------------------------------
+constexpr long MBAR_SPIN_LIMIT = 1L << 21;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// order this thread's earlier generic-proxy shared accesses before later async-proxy ones
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned* flag) {
+  for (long it = 0; it < MBAR_SPIN_LIMIT; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  raise_flag(flag, SLES_ERRF_WAIT_TIMEOUT);
+  return false;
+}
+
+// bytes must be a multiple of 16; both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
 // exp(sign * 2 pi i e / m) computed in float64 and rounded once to Tp
 template <typename Tp>
 __device__ __forceinline__ typename CT<Tp>::C twiddle(long long e, long long m, int sign) {

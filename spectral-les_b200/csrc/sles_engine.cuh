@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <mutex>
+#include <unordered_map>
 #include <unordered_set>
 
 #include "../../include/sles.h"
@@ -48,6 +49,7 @@ struct Engine {
                     cudaStream_t st) = 0;
   virtual int diag(PlanInfo& p, const void* uh, const void* uphys, double* out, double* spec, int nshell,
                    cudaStream_t st) = 0;
+  virtual int profile_rhs(PlanInfo& p, const void* uh, void* du, int iters, double* ms, cudaStream_t st) = 0;
 };
 
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? SLES_OK : SLES_ERR_CUDA; }
@@ -68,6 +70,38 @@ inline int launch(void (*kern)(KArgs...), long long grid, int block, size_t smem
       done.insert((const void*)kern);
     }
   }
+  kern<<<(unsigned)grid, block, smem, st>>>(static_cast<KArgs>(args)...);
+  return cuda_status(cudaGetLastError());
+}
+
+// Persistent launch: `work` block-sized work units, grid capped at the number
+// of blocks that can be resident at once (kernels loop over their units).
+template <typename... KArgs, typename... Args>
+inline int launch_persistent(void (*kern)(KArgs...), long long work, int block, size_t smem, cudaStream_t st,
+                             Args... args) {
+  if (work <= 0) return SLES_OK;
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> cache;
+  int resident = 0;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = cache.find((const void*)kern);
+    if (it != cache.end()) {
+      resident = it->second;
+    } else {
+      if (smem > 48 * 1024 &&
+          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return SLES_ERR_CUDA;
+      int dev = 0, nsm = 0, per = 0;
+      if (cudaGetDevice(&dev) != cudaSuccess) return SLES_ERR_CUDA;
+      if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return SLES_ERR_CUDA;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, block, smem) != cudaSuccess) return SLES_ERR_CUDA;
+      if (per < 1) return SLES_ERR_UNSUPPORTED;
+      resident = per * nsm;
+      cache[(const void*)kern] = resident;
+    }
+  }
+  const long long grid = work < resident ? work : resident;
   kern<<<(unsigned)grid, block, smem, st>>>(static_cast<KArgs>(args)...);
   return cuda_status(cudaGetLastError());
 }
@@ -114,21 +148,21 @@ struct Transforms {
       na = 1; astride = 0; pstride = p.nkp;
     }
     const long long items = (long long)nf * na * nchunks;
-    return launch(k_c2c_axis<Tp, N, G::W, G::G, DIR>, (items + G::G - 1) / G::G, K::THREADS, K::SMEM, st,
+    return launch_persistent(k_c2c_axis<Tp, N, G::W, G::G, DIR>, (items + G::G - 1) / G::G, K::THREADS, K::SMEM, st,
                   src, dst, fs, nf, na, astride, pstride, p.nk, nchunks, scale);
   }
 
   static int r2c_lines(const PlanInfo& p, const Tp* src, C* dst, int nf, cudaStream_t st) {
     using K = RealAxis<Tp, N, G::LPB>;
     const long long nlines = (long long)nf * (DIM == 3 ? (long long)N * N : N);
-    return launch(k_r2c_line<Tp, N, G::LPB>, (nlines + G::LPB - 1) / G::LPB, K::THREADS, K::SMEM, st, src,
+    return launch_persistent(k_r2c_line<Tp, N, G::LPB>, (nlines + G::LPB - 1) / G::LPB, K::THREADS, K::SMEM, st, src,
                   dst, nlines, p.nkp);
   }
 
   static int c2r_lines(const PlanInfo& p, const C* src, Tp* dst, int nf, Tp scale, cudaStream_t st) {
     using K = RealAxis<Tp, N, G::LPB>;
     const long long nlines = (long long)nf * (DIM == 3 ? (long long)N * N : N);
-    return launch(k_c2r_line<Tp, N, G::LPB>, (nlines + G::LPB - 1) / G::LPB, K::THREADS, K::SMEM, st, src,
+    return launch_persistent(k_c2r_line<Tp, N, G::LPB>, (nlines + G::LPB - 1) / G::LPB, K::THREADS, K::SMEM, st, src,
                   dst, nlines, p.nkp, scale);
   }
 
@@ -160,7 +194,7 @@ struct EngineImpl final : Engine {
   using C = typename CT<Tp>::C;
   using TR = Transforms<Tp, N, DIM>;
   using FX = typename PlanLo<Tp, N>::F;
-  using FY = typename PlanFor<Tp, N>::F;
+  using FY = typename PlanLo<Tp, N>::F;
   static constexpr int W = Cols<Tp>::W;
   static constexpr int GX = cmax(1, 256 / (W * FX::T));
   static constexpr int GY = cmax(1, 256 / (W * FY::T));
@@ -227,7 +261,7 @@ struct EngineImpl final : Engine {
   int xpass(const PlanInfo& p, const XArgs<Tp>& a, cudaStream_t st) {
     using K = XGeo<Tp, N, FX, W, GX>;
     const long long items = (long long)(DIM == 3 ? N : 1) * nchunks(p);
-    return launch(k_xpass<Tp, N, FX, W, GX, DIM, LES, PAR2D>, (items + GX - 1) / GX, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_xpass<Tp, N, FX, W, GX, DIM, LES, PAR2D>, (items + GX - 1) / GX, K::THREADS, K::SMEM, st, a);
   }
   int xpass_rt(const PlanInfo& p, const XArgs<Tp>& a, int les, int par2d, cudaStream_t st) {
     if (!les) return xpass<0, 0>(p, a, st);
@@ -241,8 +275,8 @@ struct EngineImpl final : Engine {
     using K = XGeo<Tp, N, FY, W, GY>;
     YArgs<Tp> a{slot(p, 0), p.hc_elems, p.nkp, p.nk, nchunks(p)};
     const long long items = (long long)N * nchunks(p);
-    if (inv) return launch(k_ypass_inv<Tp, N, FY, W, GY, LES>, (items + GY - 1) / GY, K::THREADS, K::SMEM, st, a);
-    return launch(k_ypass_fwd<Tp, N, FY, W, GY, LES>, (items + GY - 1) / GY, K::THREADS, K::SMEM, st, a);
+    if (inv) return launch_persistent(k_ypass_inv<Tp, N, FY, W, GY, LES>, (items + GY - 1) / GY, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_ypass_fwd<Tp, N, FY, W, GY, LES>, (items + GY - 1) / GY, K::THREADS, K::SMEM, st, a);
   }
 
   template <int LES, int MODEL, int PAR2D>
@@ -261,7 +295,9 @@ struct EngineImpl final : Engine {
     a.cphys = cphys;
     a.rs = p.real_elems;
     a.stress_only = stress_only;
-    return launch(k_zpass<Tp, N, DIM, LES, MODEL, PAR2D, LPI>, (a.nlines + LPI - 1) / LPI, K::THREADS, K::SMEM, st, a);
+    a.err = p.flags;
+    if (p.nkp != K::NKP) return SLES_ERR_INVALID_ARG;
+    return launch_persistent(k_zpass<Tp, N, DIM, LES, MODEL, PAR2D, LPI>, (a.nlines + LPI - 1) / LPI, K::THREADS, K::SMEM, st, a);
   }
   int zpass_rt(const PlanInfo& p, int les, int model, int par2d, const Tp* uphys, const Tp* cphys, int so,
                cudaStream_t st) {
@@ -378,6 +414,48 @@ struct EngineImpl final : Engine {
       }
     }
     return pipeline(p, les, (const C*)ucur, primed, (const Tp*)uphys, (const Tp*)cphys, 0, a, st);
+  }
+
+  int profile_rhs(PlanInfo& p, const void* uh, void* du, int iters, double* ms, cudaStream_t st) override {
+    const int les = p.d.les_model != SLES_LES_NONE;
+    const int model = p.d.les_model, par2d = p.d.parity;
+    cudaEvent_t ev[6];
+    for (int i = 0; i < 6; ++i)
+      if (cudaEventCreate(&ev[i]) != cudaSuccess) return SLES_ERR_CUDA;
+    double acc[5] = {0, 0, 0, 0, 0};
+    int status = SLES_OK;
+    for (int it = 0; it < iters && status == SLES_OK; ++it) {
+      XArgs<Tp> a0 = xbase(p);
+      a0.fwd = 0;
+      a0.prep = 1;
+      a0.uinv = (const C*)uh;
+      XArgs<Tp> a = xbase(p);
+      a.kind = KX_RHS;
+      a.prep = 1;
+      a.fwd = 1;
+      a.ucur = (const C*)uh;
+      a.uout = (C*)du;
+      cudaEventRecord(ev[0], st);
+      status = xpass_rt(p, a0, les, par2d, st);
+      cudaEventRecord(ev[1], st);
+      if (status == SLES_OK) status = les ? ypass<1>(p, 1, st) : ypass<0>(p, 1, st);
+      cudaEventRecord(ev[2], st);
+      if (status == SLES_OK) status = zpass_rt(p, les, model, par2d, nullptr, nullptr, 0, st);
+      cudaEventRecord(ev[3], st);
+      if (status == SLES_OK) status = les ? ypass<1>(p, 0, st) : ypass<0>(p, 0, st);
+      cudaEventRecord(ev[4], st);
+      if (status == SLES_OK) status = xpass_rt(p, a, les, par2d, st);
+      cudaEventRecord(ev[5], st);
+      if (cudaEventSynchronize(ev[5]) != cudaSuccess) status = SLES_ERR_CUDA;
+      for (int k = 0; k < 5 && status == SLES_OK; ++k) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+        acc[k] += t;
+      }
+    }
+    for (int i = 0; i < 6; ++i) cudaEventDestroy(ev[i]);
+    for (int k = 0; k < 5; ++k) ms[k] = iters > 0 ? acc[k] / iters : 0.0;
+    return status;
   }
 
   int diag(PlanInfo& p, const void* uh, const void* uphys, double* out, double* spec, int nshell,

@@ -44,22 +44,26 @@ k_c2c_axis(const typename CT<Tp>::C* src, typename CT<Tp>::C* dst,  // may alias
   const int l = tid % W, j = (tid / W) % K::T, g = tid / (W * K::T);
   typename K::F fft;
   fft.init(j);
-  const long long it = (long long)blockIdx.x * G + g;
-  const int chunk = (int)(it % nchunks);
-  const long long rest = it / nchunks;
-  const int a = (int)(rest % na);
-  const int f = (int)(rest / na);
-  const int col = chunk * W + l;
-  const bool ok = (f < nfields) && (col < ncols);
-  const long long base = (long long)f * fstride + (long long)a * astride + col;
-  C v[K::V];
+  const long long items = (long long)nfields * na * nchunks;
+  const long long nbi = (items + G - 1) / G;
+  for (long long bi = blockIdx.x; bi < nbi; bi += gridDim.x) {  // persistent over work items
+    const long long it = bi * G + g;
+    const int chunk = (int)(it % nchunks);
+    const long long rest = it / nchunks;
+    const int a = (int)(rest % na);
+    const int f = (int)(rest / na);
+    const int col = chunk * W + l;
+    const bool ok = (f < nfields) && (col < ncols);
+    const long long base = ok ? (long long)f * fstride + (long long)a * astride + col : 0;
+    C v[K::V];
 #pragma unroll
-  for (int m = 0; m < K::V; ++m)
-    v[m] = ok ? src[base + (long long)(j + K::T * m) * pstride] : cmk<C>(0, 0);
-  fft.template run<DIR>(v, j, scr + g * K::SCR + l, W);
-  if (ok) {
+    for (int m = 0; m < K::V; ++m)
+      v[m] = ok ? src[base + (long long)(j + K::T * m) * pstride] : cmk<C>(0, 0);
+    fft.template run<DIR>(v, j, scr + g * K::SCR + l, W);
+    if (ok) {
 #pragma unroll
-    for (int m = 0; m < K::V; ++m) dst[base + (long long)(j + K::T * m) * pstride] = cscale(v[m], scale);
+      for (int m = 0; m < K::V; ++m) dst[base + (long long)(j + K::T * m) * pstride] = cscale(v[m], scale);
+    }
   }
 }
 
@@ -92,17 +96,20 @@ k_r2c_line(const Tp* __restrict__ src, typename CT<Tp>::C* __restrict__ dst, lon
   const int j = tid % K::T, ln = tid / K::T;
   typename K::F fft;
   fft.init(j);
-  const long long line = (long long)blockIdx.x * LPB + ln;
-  const bool ok = line < nlines;
-  const C* in = reinterpret_cast<const C*>(src + (ok ? line : 0) * NR);
-  C* out = dst + (ok ? line : 0) * NKP;
-  C v[K::F::V];
+  const long long nbi = (nlines + LPB - 1) / LPB;
+  for (long long bi = blockIdx.x; bi < nbi; bi += gridDim.x) {
+    const long long line = bi * LPB + ln;
+    const bool ok = line < nlines;
+    const C* in = reinterpret_cast<const C*>(src + (ok ? line : 0) * NR);
+    C* out = dst + (ok ? line : 0) * NKP;
+    C v[K::F::V];
 #pragma unroll
-  for (int m = 0; m < K::F::V; ++m) v[m] = ok ? in[j + K::T * m] : cmk<C>(0, 0);
-  fft.template run<-1>(v, j, scr + ln * K::LS, 1);
-  r2c_post<typename K::F>(v, j, scr + ln * K::LS, 1, twN, [&](int k, C x) {
-    if (ok) out[k] = x;
-  });
+    for (int m = 0; m < K::F::V; ++m) v[m] = ok ? in[j + K::T * m] : cmk<C>(0, 0);
+    fft.template run<-1>(v, j, scr + ln * K::LS, 1);
+    r2c_post<typename K::F>(v, j, scr + ln * K::LS, 1, twN, [&](int k, C x) {
+      if (ok) out[k] = x;
+    });
+  }
 }
 
 template <typename Tp, int NR, int LPB>
@@ -120,16 +127,19 @@ k_c2r_line(const typename CT<Tp>::C* __restrict__ src, Tp* __restrict__ dst, lon
   const int j = tid % K::T, ln = tid / K::T;
   typename K::F fft;
   fft.init(j);
-  const long long line = (long long)blockIdx.x * LPB + ln;
-  const bool ok = line < nlines;
-  const C* in = src + (ok ? line : 0) * NKP;
-  C* out = reinterpret_cast<C*>(dst + (ok ? line : 0) * NR);
-  C v[K::F::V];
-  c2r_pre<typename K::F>(v, j, twN, [&](int k) { return ok ? in[k] : cmk<C>(0, 0); });
-  fft.template run<+1>(v, j, scr + ln * K::LS, 1);
-  if (ok) {
+  const long long nbi = (nlines + LPB - 1) / LPB;
+  for (long long bi = blockIdx.x; bi < nbi; bi += gridDim.x) {
+    const long long line = bi * LPB + ln;
+    const bool ok = line < nlines;
+    const C* in = src + (ok ? line : 0) * NKP;
+    C* out = reinterpret_cast<C*>(dst + (ok ? line : 0) * NR);
+    C v[K::F::V];
+    c2r_pre<typename K::F>(v, j, twN, [&](int k) { return ok ? in[k] : cmk<C>(0, 0); });
+    fft.template run<+1>(v, j, scr + ln * K::LS, 1);
+    if (ok) {
 #pragma unroll
-    for (int m = 0; m < K::F::V; ++m) out[j + K::T * m] = cscale(v[m], scale);
+      for (int m = 0; m < K::F::V; ++m) out[j + K::T * m] = cscale(v[m], scale);
+    }
   }
 }
 

@@ -190,11 +190,13 @@ __device__ __forceinline__ void combine_update(const XArgs<Tp>& A, typename CT<T
 template <typename Tp, int N, class F, int W, int G>
 struct XGeo {
   static constexpr int T = F::T, V = F::V, THREADS = G * W * T, SCR = xline_len(N) * W;
+  // resident blocks per SM the register allocation must allow
+  static constexpr int MINB = (THREADS >= 512) ? 1 : (sizeof(Tp) == 4 ? 2 : 1);
   static constexpr size_t SMEM = (size_t)G * SCR * sizeof(typename CT<Tp>::C);
 };
 
 template <typename Tp, int N, class F, int W, int G, int DIM, int LES, int PAR2D>
-__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS) k_xpass(const XArgs<Tp> A) {
+__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS, XGeo<Tp, N, F, W, G>::MINB) k_xpass(const XArgs<Tp> A) {
   using K = XGeo<Tp, N, F, W, G>;
   using C = typename CT<Tp>::C;
   constexpr int T = K::T, V = K::V, D = DIM;
@@ -204,129 +206,134 @@ __global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS) k_xpass(const X
   const int l = tid % W, j = (tid / W) % T, g = tid / (W * T);
   F fft;
   fft.init(j);
-  const long long it = (long long)blockIdx.x * G + g;
-  const int chunk = (int)(it % A.nchunks);
-  const int sl = (int)(it / A.nchunks);            // ky slice (3D); 0 in 2D
-  const int nsl = (DIM == 3) ? N : 1;
-  const int col = chunk * W + l;
-  const bool ok = sl < nsl && col < A.nk;
-  const long long base = (long long)(sl < nsl ? sl : 0) * A.nkp + col;
-  const long long ps = (DIM == 3) ? (long long)N * A.nkp : (long long)A.nkp;
-  const long long fs = A.fs;
-  C* sm = scr + g * K::SCR + l;
-  C* ws = A.ws;
-  auto ld = [&](const C* f, C (&v)[V]) {
+  const long long items_ = (long long)((DIM == 3) ? N : 1) * A.nchunks;
+  const long long nbi_ = (items_ + G - 1) / G;
+  for (long long bi = blockIdx.x; bi < nbi_; bi += gridDim.x) {  // persistent over work items
+    const long long it = bi * G + g;
+    const int chunk = (int)(it % A.nchunks);
+    const int sl = (int)(it / A.nchunks);            // ky slice (3D); 0 in 2D
+    const int nsl = (DIM == 3) ? N : 1;
+    const int col = chunk * W + l;
+    const bool ok = sl < nsl && col < A.nk;
+    const long long base = (long long)(sl < nsl ? sl : 0) * A.nkp + col;
+    const long long ps = (DIM == 3) ? (long long)N * A.nkp : (long long)A.nkp;
+    const long long fs = A.fs;
+    C* sm = scr + g * K::SCR + l;
+    C* ws = A.ws;
+    auto ld = [&](const C* f, C (&v)[V]) {
 #pragma unroll
-    for (int m = 0; m < V; ++m) v[m] = ok ? f[base + (j + T * m) * ps] : cmk<C>(0, 0);
-  };
-  auto st = [&](int slot, const C (&v)[V]) {
-    if (ok) {
+      for (int m = 0; m < V; ++m) v[m] = ok ? f[base + (j + T * m) * ps] : cmk<C>(0, 0);
+    };
+    auto st = [&](int slot, const C (&v)[V]) {
+      if (ok) {
 #pragma unroll
-      for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
-    }
-  };
-  auto kx_at = [&](int m) { return kc2c(j + T * m, N); };
-  C S[D][V];
-  if (A.fwd) {
-    if (DIM == 3) {
+        for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
+      }
+    };
+    auto kx_at = [&](int m) { return kc2c(j + T * m, N); };
+    C S[D][V];
+    if (A.fwd) {
+      if (DIM == 3) {
 #pragma unroll
-      for (int c = 0; c < D; ++c) {
-        ld(ws + c * fs, S[c]);
-        fft.template run<-1>(S[c], j, sm, W);
-        if (LES) {  // + 2i kx F_cx
+        for (int c = 0; c < D; ++c) {
+          ld(ws + c * fs, S[c]);
+          fft.template run<-1>(S[c], j, sm, W);
+          if (LES) {  // + 2i kx F_cx
+            C h[V];
+            ld(ws + (3 + c) * fs, h);
+            fft.template run<-1>(h, j, sm, W);
+#pragma unroll
+            for (int m = 0; m < V; ++m) S[c][m] = cadd(S[c][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+          }
+        }
+      } else {
+        const Tp ky2 = (Tp)(2 * col);
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+          ld(ws + c * fs, S[c]);
+          fft.template run<-1>(S[c], j, sm, W);
+        }
+        if (LES) {
+          // reference (math_formula.py:128-146): T_0 = 2i(kx F12 + ky F22), T_1 = 0
+          // corrected: T_0 = 2i(kx F11 + ky F12), T_1 = 2i(kx F12 + ky F22)
           C h[V];
-          ld(ws + (3 + c) * fs, h);
+          ld(ws + 2 * fs, h);
           fft.template run<-1>(h, j, sm, W);
 #pragma unroll
-          for (int m = 0; m < V; ++m) S[c][m] = cadd(S[c][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+          for (int m = 0; m < V; ++m) S[0][m] = cadd(S[0][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+          ld(ws + 3 * fs, h);
+          fft.template run<-1>(h, j, sm, W);
+#pragma unroll
+          for (int m = 0; m < V; ++m) {
+            S[0][m] = cadd(S[0][m], cmuli_s(h[m], ky2));
+            if (!PAR2D) S[1][m] = cadd(S[1][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+          }
+          if (!PAR2D) {
+            ld(ws + 4 * fs, h);
+            fft.template run<-1>(h, j, sm, W);
+#pragma unroll
+            for (int m = 0; m < V; ++m) S[1][m] = cadd(S[1][m], cmuli_s(h[m], ky2));
+          }
+        }
+      }
+      if (ok) {
+#pragma unroll
+        for (int m = 0; m < V; ++m) {
+          C s[D];
+          int k[D];
+#pragma unroll
+          for (int c = 0; c < D; ++c) s[c] = S[c][m];
+          k[0] = kx_at(m);
+          if (DIM == 3) { k[1] = kc2c(sl, N); k[D - 1] = col; }
+          else k[1] = col;
+          combine_update<Tp, D>(A, s, k, base + (j + T * m) * ps);
+#pragma unroll
+          for (int c = 0; c < D; ++c) S[c][m] = s[c];
         }
       }
     } else {
-      const Tp ky2 = (Tp)(2 * col);
 #pragma unroll
-      for (int c = 0; c < D; ++c) {
-        ld(ws + c * fs, S[c]);
-        fft.template run<-1>(S[c], j, sm, W);
-      }
+      for (int c = 0; c < D; ++c) ld(A.uinv + c * fs, S[c]);
+    }
+    if (A.prep) {  // uniform across the block
       if (LES) {
-        // reference (math_formula.py:128-146): T_0 = 2i(kx F12 + ky F22), T_1 = 0
-        // corrected: T_0 = 2i(kx F11 + ky F12), T_1 = 2i(kx F12 + ky F22)
-        C h[V];
-        ld(ws + 2 * fs, h);
-        fft.template run<-1>(h, j, sm, W);
 #pragma unroll
-        for (int m = 0; m < V; ++m) S[0][m] = cadd(S[0][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
-        ld(ws + 3 * fs, h);
-        fft.template run<-1>(h, j, sm, W);
+        for (int c = 0; c < D; ++c) {
+          C b[V];
 #pragma unroll
-        for (int m = 0; m < V; ++m) {
-          S[0][m] = cadd(S[0][m], cmuli_s(h[m], ky2));
-          if (!PAR2D) S[1][m] = cadd(S[1][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+          for (int m = 0; m < V; ++m) b[m] = cmuli_s(S[c][m], (Tp)kx_at(m));
+          fft.template run<+1>(b, j, sm, W);
+          st(D + c, b);
+          fft.template run<+1>(S[c], j, sm, W);
+          st(c, S[c]);
         }
-        if (!PAR2D) {
-          ld(ws + 4 * fs, h);
-          fft.template run<-1>(h, j, sm, W);
+      } else if (DIM == 3) {
+        C q[V];
 #pragma unroll
-          for (int m = 0; m < V; ++m) S[1][m] = cadd(S[1][m], cmuli_s(h[m], ky2));
+        for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[2][m], -(Tp)kx_at(m));  // -i kx w
+        fft.template run<+1>(q, j, sm, W);
+        st(3, q);
+#pragma unroll
+        for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[1][m], (Tp)kx_at(m));   //  i kx v
+        fft.template run<+1>(q, j, sm, W);
+        st(4, q);
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+          fft.template run<+1>(S[c], j, sm, W);
+          st(c, S[c]);
+        }
+      } else {
+        C q[V];
+#pragma unroll
+        for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[1][m], (Tp)kx_at(m));   //  i kx v
+        fft.template run<+1>(q, j, sm, W);
+        st(2, q);
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+          fft.template run<+1>(S[c], j, sm, W);
+          st(c, S[c]);
         }
       }
-    }
-    if (ok) {
-#pragma unroll
-      for (int m = 0; m < V; ++m) {
-        C s[D];
-        int k[D];
-#pragma unroll
-        for (int c = 0; c < D; ++c) s[c] = S[c][m];
-        k[0] = kx_at(m);
-        if (DIM == 3) { k[1] = kc2c(sl, N); k[D - 1] = col; }
-        else k[1] = col;
-        combine_update<Tp, D>(A, s, k, base + (j + T * m) * ps);
-#pragma unroll
-        for (int c = 0; c < D; ++c) S[c][m] = s[c];
-      }
-    }
-  } else {
-#pragma unroll
-    for (int c = 0; c < D; ++c) ld(A.uinv + c * fs, S[c]);
-  }
-  if (!A.prep) return;  // uniform across the block
-  if (LES) {
-#pragma unroll
-    for (int c = 0; c < D; ++c) {
-      C b[V];
-#pragma unroll
-      for (int m = 0; m < V; ++m) b[m] = cmuli_s(S[c][m], (Tp)kx_at(m));
-      fft.template run<+1>(b, j, sm, W);
-      st(D + c, b);
-      fft.template run<+1>(S[c], j, sm, W);
-      st(c, S[c]);
-    }
-  } else if (DIM == 3) {
-    C q[V];
-#pragma unroll
-    for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[2][m], -(Tp)kx_at(m));  // -i kx w
-    fft.template run<+1>(q, j, sm, W);
-    st(3, q);
-#pragma unroll
-    for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[1][m], (Tp)kx_at(m));   //  i kx v
-    fft.template run<+1>(q, j, sm, W);
-    st(4, q);
-#pragma unroll
-    for (int c = 0; c < D; ++c) {
-      fft.template run<+1>(S[c], j, sm, W);
-      st(c, S[c]);
-    }
-  } else {
-    C q[V];
-#pragma unroll
-    for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[1][m], (Tp)kx_at(m));   //  i kx v
-    fft.template run<+1>(q, j, sm, W);
-    st(2, q);
-#pragma unroll
-    for (int c = 0; c < D; ++c) {
-      fft.template run<+1>(S[c], j, sm, W);
-      st(c, S[c]);
     }
   }
 }
@@ -343,7 +350,7 @@ struct YArgs {
 };
 
 template <typename Tp, int N, class F, int W, int G, int LES>
-__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS) k_ypass_inv(const YArgs<Tp> A) {
+__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS, XGeo<Tp, N, F, W, G>::MINB) k_ypass_inv(const YArgs<Tp> A) {
   using K = XGeo<Tp, N, F, W, G>;
   using C = typename CT<Tp>::C;
   constexpr int T = K::T, V = K::V;
@@ -353,69 +360,73 @@ __global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS) k_ypass_inv(con
   const int l = tid % W, j = (tid / W) % T, g = tid / (W * T);
   F fft;
   fft.init(j);
-  const long long it = (long long)blockIdx.x * G + g;
-  const int chunk = (int)(it % A.nchunks);
-  const int x = (int)(it / A.nchunks);
-  const int col = chunk * W + l;
-  const bool ok = x < N && col < A.nk;
-  const long long base = (long long)(x < N ? x : 0) * N * A.nkp + col;
-  const long long ps = A.nkp, fs = A.fs;
-  C* sm = scr + g * K::SCR + l;
-  C* ws = A.ws;
-  auto ld = [&](int slot, C (&v)[V]) {
+  const long long items_ = (long long)N * A.nchunks;
+  const long long nbi_ = (items_ + G - 1) / G;
+  for (long long bi = blockIdx.x; bi < nbi_; bi += gridDim.x) {  // persistent over work items
+    const long long it = bi * G + g;
+    const int chunk = (int)(it % A.nchunks);
+    const int x = (int)(it / A.nchunks);
+    const int col = chunk * W + l;
+    const bool ok = x < N && col < A.nk;
+    const long long base = (long long)(x < N ? x : 0) * N * A.nkp + col;
+    const long long ps = A.nkp, fs = A.fs;
+    C* sm = scr + g * K::SCR + l;
+    C* ws = A.ws;
+    auto ld = [&](int slot, C (&v)[V]) {
 #pragma unroll
-    for (int m = 0; m < V; ++m) v[m] = ok ? ws[slot * fs + base + (j + T * m) * ps] : cmk<C>(0, 0);
-  };
-  auto st = [&](int slot, const C (&v)[V]) {
-    if (ok) {
+      for (int m = 0; m < V; ++m) v[m] = ok ? ws[slot * fs + base + (j + T * m) * ps] : cmk<C>(0, 0);
+    };
+    auto st = [&](int slot, const C (&v)[V]) {
+      if (ok) {
 #pragma unroll
-      for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
-    }
-  };
-  auto iky = [&](const C (&v)[V], C (&w)[V]) {
+        for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
+      }
+    };
+    auto iky = [&](const C (&v)[V], C (&w)[V]) {
 #pragma unroll
-    for (int m = 0; m < V; ++m) w[m] = cmuli_s(v[m], (Tp)kc2c(j + T * m, N));
-  };
-  C v[V], w[V];
-  if (LES) {
+      for (int m = 0; m < V; ++m) w[m] = cmuli_s(v[m], (Tp)kc2c(j + T * m, N));
+    };
+    C v[V], w[V];
+    if (LES) {
 #pragma unroll 1
-    for (int c = 0; c < 3; ++c) {
-      ld(c, v);
+      for (int c = 0; c < 3; ++c) {
+        ld(c, v);
+        iky(v, w);
+        fft.template run<+1>(v, j, sm, W);
+        st(c, v);
+        fft.template run<+1>(w, j, sm, W);
+        st(6 + c, w);
+        ld(3 + c, v);
+        fft.template run<+1>(v, j, sm, W);
+        st(3 + c, v);
+      }
+    } else {
+      ld(2, v);  // A_w -> a_w and Ox = Y^-1(i ky A_w)
       iky(v, w);
       fft.template run<+1>(v, j, sm, W);
-      st(c, v);
+      st(2, v);
       fft.template run<+1>(w, j, sm, W);
-      st(6 + c, w);
-      ld(3 + c, v);
-      fft.template run<+1>(v, j, sm, W);
-      st(3 + c, v);
-    }
-  } else {
-    ld(2, v);  // A_w -> a_w and Ox = Y^-1(i ky A_w)
-    iky(v, w);
-    fft.template run<+1>(v, j, sm, W);
-    st(2, v);
-    fft.template run<+1>(w, j, sm, W);
-    st(5, w);
-    ld(0, v);  // A_u -> a_u and Oz = Y^-1(Q_z - i ky A_u)
-    ld(4, w);
+      st(5, w);
+      ld(0, v);  // A_u -> a_u and Oz = Y^-1(Q_z - i ky A_u)
+      ld(4, w);
 #pragma unroll
-    for (int m = 0; m < V; ++m) w[m] = csub(w[m], cmuli_s(v[m], (Tp)kc2c(j + T * m, N)));
-    fft.template run<+1>(v, j, sm, W);
-    st(0, v);
-    fft.template run<+1>(w, j, sm, W);
-    st(4, w);
-    ld(1, v);
-    fft.template run<+1>(v, j, sm, W);
-    st(1, v);
-    ld(3, v);
-    fft.template run<+1>(v, j, sm, W);
-    st(3, v);
+      for (int m = 0; m < V; ++m) w[m] = csub(w[m], cmuli_s(v[m], (Tp)kc2c(j + T * m, N)));
+      fft.template run<+1>(v, j, sm, W);
+      st(0, v);
+      fft.template run<+1>(w, j, sm, W);
+      st(4, w);
+      ld(1, v);
+      fft.template run<+1>(v, j, sm, W);
+      st(1, v);
+      ld(3, v);
+      fft.template run<+1>(v, j, sm, W);
+      st(3, v);
+    }
   }
 }
 
 template <typename Tp, int N, class F, int W, int G, int LES>
-__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS) k_ypass_fwd(const YArgs<Tp> A) {
+__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS, XGeo<Tp, N, F, W, G>::MINB) k_ypass_fwd(const YArgs<Tp> A) {
   using K = XGeo<Tp, N, F, W, G>;
   using C = typename CT<Tp>::C;
   constexpr int T = K::T, V = K::V;
@@ -425,83 +436,87 @@ __global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS) k_ypass_fwd(con
   const int l = tid % W, j = (tid / W) % T, g = tid / (W * T);
   F fft;
   fft.init(j);
-  const long long it = (long long)blockIdx.x * G + g;
-  const int chunk = (int)(it % A.nchunks);
-  const int x = (int)(it / A.nchunks);
-  const int col = chunk * W + l;
-  const bool ok = x < N && col < A.nk;
-  const long long base = (long long)(x < N ? x : 0) * N * A.nkp + col;
-  const long long ps = A.nkp, fs = A.fs;
-  C* sm = scr + g * K::SCR + l;
-  C* ws = A.ws;
-  auto ld = [&](int slot, C (&v)[V]) {
+  const long long items_ = (long long)N * A.nchunks;
+  const long long nbi_ = (items_ + G - 1) / G;
+  for (long long bi = blockIdx.x; bi < nbi_; bi += gridDim.x) {  // persistent over work items
+    const long long it = bi * G + g;
+    const int chunk = (int)(it % A.nchunks);
+    const int x = (int)(it / A.nchunks);
+    const int col = chunk * W + l;
+    const bool ok = x < N && col < A.nk;
+    const long long base = (long long)(x < N ? x : 0) * N * A.nkp + col;
+    const long long ps = A.nkp, fs = A.fs;
+    C* sm = scr + g * K::SCR + l;
+    C* ws = A.ws;
+    auto ld = [&](int slot, C (&v)[V]) {
 #pragma unroll
-    for (int m = 0; m < V; ++m) v[m] = ok ? ws[slot * fs + base + (j + T * m) * ps] : cmk<C>(0, 0);
-  };
-  auto st = [&](int slot, const C (&v)[V]) {
-    if (ok) {
+      for (int m = 0; m < V; ++m) v[m] = ok ? ws[slot * fs + base + (j + T * m) * ps] : cmk<C>(0, 0);
+    };
+    auto st = [&](int slot, const C (&v)[V]) {
+      if (ok) {
 #pragma unroll
-      for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
-    }
-  };
-  if (!LES) {
-    C v[V];
+        for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
+      }
+    };
+    if (!LES) {
+      C v[V];
 #pragma unroll 1
-    for (int c = 0; c < 3; ++c) {
-      ld(c, v);
-      fft.template run<-1>(v, j, sm, W);
-      st(c, v);
+      for (int c = 0; c < 3; ++c) {
+        ld(c, v);
+        fft.template run<-1>(v, j, sm, W);
+        st(c, v);
+      }
+      continue;
     }
-    return;
+    const Tp kz2 = (Tp)(2 * col);
+    auto ky2 = [&](int m) { return (Tp)(2 * kc2c(j + T * m, N)); };
+    C t[V], acc[V], acc2[V];
+    // G_x = N_x + 2i(ky F_xy + kz F_xz);  H_y = F_xy, H_z = F_xz, H_x = F_xx
+    ld(4, t);
+    fft.template run<-1>(t, j, sm, W);
+    st(4, t);
+#pragma unroll
+    for (int m = 0; m < V; ++m) acc[m] = cmuli_s(t[m], ky2(m));
+    ld(5, t);
+    fft.template run<-1>(t, j, sm, W);
+    st(5, t);
+#pragma unroll
+    for (int m = 0; m < V; ++m) acc[m] = cadd(acc[m], cmuli_s(t[m], kz2));
+    ld(0, t);
+    fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+    for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc[m]);
+    st(0, t);
+    ld(3, t);
+    fft.template run<-1>(t, j, sm, W);
+    st(3, t);
+    // G_y = N_y + 2i(ky F_yy + kz F_yz);  G_z = N_z + 2i(ky F_yz + kz F_zz)
+    ld(6, t);
+    fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+    for (int m = 0; m < V; ++m) acc[m] = cmuli_s(t[m], ky2(m));
+    ld(7, t);
+    fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+    for (int m = 0; m < V; ++m) {
+      acc[m] = cadd(acc[m], cmuli_s(t[m], kz2));
+      acc2[m] = cmuli_s(t[m], ky2(m));
+    }
+    ld(1, t);
+    fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+    for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc[m]);
+    st(1, t);
+    ld(8, t);
+    fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+    for (int m = 0; m < V; ++m) acc2[m] = cadd(acc2[m], cmuli_s(t[m], kz2));
+    ld(2, t);
+    fft.template run<-1>(t, j, sm, W);
+#pragma unroll
+    for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc2[m]);
+    st(2, t);
   }
-  const Tp kz2 = (Tp)(2 * col);
-  auto ky2 = [&](int m) { return (Tp)(2 * kc2c(j + T * m, N)); };
-  C t[V], acc[V], acc2[V];
-  // G_x = N_x + 2i(ky F_xy + kz F_xz);  H_y = F_xy, H_z = F_xz, H_x = F_xx
-  ld(4, t);
-  fft.template run<-1>(t, j, sm, W);
-  st(4, t);
-#pragma unroll
-  for (int m = 0; m < V; ++m) acc[m] = cmuli_s(t[m], ky2(m));
-  ld(5, t);
-  fft.template run<-1>(t, j, sm, W);
-  st(5, t);
-#pragma unroll
-  for (int m = 0; m < V; ++m) acc[m] = cadd(acc[m], cmuli_s(t[m], kz2));
-  ld(0, t);
-  fft.template run<-1>(t, j, sm, W);
-#pragma unroll
-  for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc[m]);
-  st(0, t);
-  ld(3, t);
-  fft.template run<-1>(t, j, sm, W);
-  st(3, t);
-  // G_y = N_y + 2i(ky F_yy + kz F_yz);  G_z = N_z + 2i(ky F_yz + kz F_zz)
-  ld(6, t);
-  fft.template run<-1>(t, j, sm, W);
-#pragma unroll
-  for (int m = 0; m < V; ++m) acc[m] = cmuli_s(t[m], ky2(m));
-  ld(7, t);
-  fft.template run<-1>(t, j, sm, W);
-#pragma unroll
-  for (int m = 0; m < V; ++m) {
-    acc[m] = cadd(acc[m], cmuli_s(t[m], kz2));
-    acc2[m] = cmuli_s(t[m], ky2(m));
-  }
-  ld(1, t);
-  fft.template run<-1>(t, j, sm, W);
-#pragma unroll
-  for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc[m]);
-  st(1, t);
-  ld(8, t);
-  fft.template run<-1>(t, j, sm, W);
-#pragma unroll
-  for (int m = 0; m < V; ++m) acc2[m] = cadd(acc2[m], cmuli_s(t[m], kz2));
-  ld(2, t);
-  fft.template run<-1>(t, j, sm, W);
-#pragma unroll
-  for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc2[m]);
-  st(2, t);
 }
 
 // ---------------------------------------------------------------------------
@@ -522,18 +537,31 @@ struct ZArgs {
   const Tp* cphys;       // optional stored curl (3 real fields in 3D, 1 in 2D)
   long long rs;          // elements per real field
   int stress_only;       // 1: drop u x omega (evaluates the LES stress alone)
+  unsigned* err;         // error word (bounded-wait timeouts)
 };
 
 template <typename Tp, int N, int DIM, int LES, int PAR2D, int LPI>
 struct ZGeo {
   using F = typename PlanFor<Tp, N / 2>::F;
+  using C = typename CT<Tp>::C;
   static constexpr int L = N / 2, T = F::T, V = F::V;
-  static constexpr int NG = (DIM == 3) ? (LES ? 12 : 6) : (LES ? 6 : 3);
+  static constexpr int NG = (DIM == 3) ? (LES ? 12 : 6) : (LES ? 6 : 3);    // physical fields
+  static constexpr int NIN = (DIM == 3) ? (LES ? 9 : 6) : (LES ? 4 : 3);    // input slots
   static constexpr int NOUT = (DIM == 3) ? (LES ? 9 : 3) : (LES ? (PAR2D ? 4 : 5) : 2);
+  static constexpr int NKP = ((N / 2 + 1) + 3) / 4 * 4;
   static constexpr int THREADS = NG * LPI * T;
+  static constexpr int MINB = (sizeof(Tp) == 4) ? (THREADS <= 192 ? 3 : 2) : 1;
+  // per (field, line) region: the line's FFT exchange scratch (LS complex,
+  // LS = 8 mod 16 keeps the autosort writes conflict-free) and, between the
+  // transforms, the physical line itself (N reals)
   static constexpr int LS = ((xline_len(L) + 15) / 16) * 16 + 8;
-  static constexpr size_t SMEM =
-      ((size_t)L + (size_t)NG * LPI * LS) * sizeof(typename CT<Tp>::C) + (size_t)NG * LPI * N * sizeof(Tp);
+  static constexpr int RS = 2 * LS;
+  static_assert(RS >= N, "region must hold a physical line");
+  static constexpr int STAGE = NIN * LPI * NKP;   // complex elements per staging buffer
+  static constexpr size_t OFF_TW = 16;
+  static constexpr size_t OFF_STAGE = OFF_TW + (size_t)L * sizeof(C);
+  static constexpr size_t OFF_REG = OFF_STAGE + 2 * (size_t)STAGE * sizeof(C);
+  static constexpr size_t SMEM = OFF_REG + (size_t)NG * LPI * RS * sizeof(Tp);
 };
 
 template <typename Tp, int MODEL>
@@ -628,101 +656,129 @@ __device__ __forceinline__ void z_pointwise(Tp* st, int ps, int p, const Tp* uo,
 }
 
 template <typename Tp, int N, int DIM, int LES, int MODEL, int PAR2D, int LPI>
-__global__ void __launch_bounds__(ZGeo<Tp, N, DIM, LES, PAR2D, LPI>::THREADS) k_zpass(const ZArgs<Tp> A) {
+__global__ void __launch_bounds__(ZGeo<Tp, N, DIM, LES, PAR2D, LPI>::THREADS, ZGeo<Tp, N, DIM, LES, PAR2D, LPI>::MINB)
+k_zpass(const ZArgs<Tp> A) {
   using K = ZGeo<Tp, N, DIM, LES, PAR2D, LPI>;
   using F = typename K::F;
   using C = typename CT<Tp>::C;
-  constexpr int T = K::T, V = K::V, L = K::L;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* twN = reinterpret_cast<C*>(smem_raw);
-  C* scr = twN + L;
-  Tp* stash = reinterpret_cast<Tp*>(scr + K::NG * LPI * K::LS);
-  constexpr int PS = LPI * N;  // stash field stride
-  fill_twN<Tp, N>(twN);
-  __syncthreads();
+  constexpr int T = K::T, V = K::V, NKP = K::NKP, SFS = LPI * K::RS;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
+  C* twN = reinterpret_cast<C*>(smem_raw + K::OFF_TW);
+  C* stage = reinterpret_cast<C*>(smem_raw + K::OFF_STAGE);   // [2][NIN][LPI][NKP]
+  Tp* reg = reinterpret_cast<Tp*>(smem_raw + K::OFF_REG);     // [NG][LPI][RS]
   const int tid = threadIdx.x;
+  fill_twN<Tp, N>(twN);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
   const int j = tid % T, ln = (tid / T) % LPI, grp = tid / (T * LPI);
   F fft;
   fft.init(j);
-  const long long line0 = (long long)blockIdx.x * LPI;
-  const long long line = line0 + ln;
-  const bool ok = line < A.nlines;
-  const long long lo = (ok ? line : 0) * A.nkp;
   const long long fs = A.fs;
-  C* sm = scr + (grp * LPI + ln) * K::LS;
-  const C* ws = A.ws;
-  // ---- phase A: c2r of physical field `grp` = slot s1 + sgn * i k * slot s2
-  {
-    int s1 = grp, s2 = -1;
-    Tp sgn = 0;
-    if (DIM == 3) {
-      if (LES) {
-        if (grp >= 9) { s1 = -1; s2 = grp - 9; sgn = 1; }      // d/dz u_c = i kz a_c
-      } else {
-        if (grp == 3) { s1 = 5; s2 = 1; sgn = -1; }             // omega_x = Ox - i kz v
-        else if (grp == 4) { s1 = 3; s2 = 0; sgn = 1; }         // omega_y = Oy + i kz u
-        else if (grp == 5) { s1 = 4; }                          // omega_z = Oz
-      }
+  Tp* myreg = reg + (grp * LPI + ln) * K::RS;
+  C* sm = reinterpret_cast<C*>(myreg);
+  // physical field `grp` = slot s1 + sgn * i k * slot s2  (k: r2c-axis wavenumber)
+  int s1 = grp, s2 = -1;
+  Tp sgn = 0;
+  if (DIM == 3) {
+    if (LES) {
+      if (grp >= 9) { s1 = -1; s2 = grp - 9; sgn = 1; }      // d/dz u_c = i kz a_c
     } else {
-      if (LES) {
-        if (grp == 4) { s1 = -1; s2 = 0; sgn = 1; }             // a21 = du/dy
-        else if (grp == 5) { s1 = -1; s2 = 1; sgn = 1; }        // a22 = dv/dy
-      } else if (grp == 2) {
-        s1 = 2; s2 = 0; sgn = -1;                               // omega = X^-1(i kx v) - i ky u
+      if (grp == 3) { s1 = 5; s2 = 1; sgn = -1; }             // omega_x = Ox - i kz v
+      else if (grp == 4) { s1 = 3; s2 = 0; sgn = 1; }         // omega_y = Oy + i kz u
+      else if (grp == 5) { s1 = 4; }                          // omega_z = Oz
+    }
+  } else {
+    if (LES) {
+      if (grp == 4) { s1 = -1; s2 = 0; sgn = 1; }             // a21 = du/dy
+      else if (grp == 5) { s1 = -1; s2 = 1; sgn = 1; }        // a22 = dv/dy
+    } else if (grp == 2) {
+      s1 = 2; s2 = 0; sgn = -1;                               // omega = X^-1(i kx v) - i ky u
+    }
+  }
+  const long long nbi = (A.nlines + LPI - 1) / LPI;
+  // thread 0 stages the NIN input slots of line group `b` into buffer `buf`
+  auto issue = [&](long long b, int buf) {
+    const long long l0 = b * LPI;
+    const long long nl = (A.nlines - l0 < LPI) ? A.nlines - l0 : LPI;
+    const unsigned bytes = (unsigned)(nl * A.nkp * (long long)sizeof(C));
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&bar[buf], bytes * K::NIN);
+    for (int s = 0; s < K::NIN; ++s)
+      bulk_g2s(stage + buf * K::STAGE + s * LPI * NKP, A.ws + s * fs + l0 * A.nkp, bytes, &bar[buf]);
+  };
+  if (tid == 0 && blockIdx.x < nbi) issue(blockIdx.x, 0);
+  int iter = 0;
+  for (long long bi = blockIdx.x; bi < nbi; bi += gridDim.x, ++iter) {  // persistent over line groups
+    const int buf = iter & 1;
+    if (tid == 0 && bi + gridDim.x < nbi) issue(bi + gridDim.x, buf ^ 1);
+    mbar_wait_bounded(&bar[buf], (iter >> 1) & 1, A.err);
+    const long long line0 = bi * LPI;
+    const long long line = line0 + ln;
+    const bool ok = line < A.nlines;
+    const long long lo = (ok ? line : 0) * A.nkp;
+    // ---- phase A: c2r of physical field `grp` from the staged slots
+    {
+      const C* sb = stage + buf * K::STAGE + ln * NKP;
+      C v[V];
+      c2r_pre<F>(v, j, twN, [&](int k) {
+        C r = cmk<C>(0, 0);
+        if (!ok) return r;
+        if (s1 >= 0) r = sb[s1 * LPI * NKP + k];
+        if (s2 >= 0) r = cadd(r, cmuli_s(sb[s2 * LPI * NKP + k], sgn * (Tp)k));
+        return r;
+      });
+      fft.template run<+1>(v, j, sm, 1);
+      __syncthreads();  // the region doubles as exchange scratch: all reads done
+      C* dst = reinterpret_cast<C*>(myreg);
+#pragma unroll
+      for (int m = 0; m < V; ++m) dst[j + T * m] = cscale(v[m], A.scale);
+    }
+    __syncthreads();
+    // ---- phase B: pointwise products
+    for (int p = tid; p < LPI * N; p += K::THREADS) {
+      const int pln = p / N, z = p % N;
+      const long long pl = line0 + pln;
+      if (pl >= A.nlines) continue;
+      const long long o = pl * N + z;
+      Tp ub[3], cb[3];
+      const Tp* uo = nullptr;
+      const Tp* co = nullptr;
+      if (A.uphys) {
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) ub[c] = A.uphys[c * A.rs + o];
+        uo = ub;
+      }
+      if (A.cphys) {
+#pragma unroll
+        for (int c = 0; c < (DIM == 3 ? 3 : 1); ++c) cb[c] = A.cphys[c * A.rs + o];
+        co = cb;
+      }
+      const int sp = pln * K::RS + z;
+      z_pointwise<Tp, DIM, LES, MODEL, PAR2D>(reg, SFS, sp, uo, co, A.cdx2);
+      if (A.stress_only) {
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) reg[c * SFS + sp] = (Tp)0;
       }
     }
-    C v[V];
-    c2r_pre<F>(v, j, twN, [&](int k) {
-      C r = cmk<C>(0, 0);
-      if (!ok) return r;
-      if (s1 >= 0) r = ws[s1 * fs + lo + k];
-      if (s2 >= 0) r = cadd(r, cmuli_s(ws[s2 * fs + lo + k], sgn * (Tp)k));
-      return r;
-    });
-    fft.template run<+1>(v, j, sm, 1);
-    C* dst = reinterpret_cast<C*>(stash + grp * PS + ln * N);
+    __syncthreads();
+    // ---- phase C: r2c of product `grp` (groups >= NOUT run idle for the barriers)
+    {
+      C v[V];
+      const C* src = reinterpret_cast<const C*>(myreg);
 #pragma unroll
-    for (int m = 0; m < V; ++m) dst[j + T * m] = cscale(v[m], A.scale);
-  }
-  __syncthreads();
-  // ---- phase B: pointwise products
-  for (int p = tid; p < PS; p += K::THREADS) {
-    const long long pl = line0 + p / N;
-    if (pl >= A.nlines) continue;
-    const long long o = pl * N + (p % N);
-    Tp ub[3], cb[3];
-    const Tp* uo = nullptr;
-    const Tp* co = nullptr;
-    if (A.uphys) {
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) ub[c] = A.uphys[c * A.rs + o];
-      uo = ub;
+      for (int m = 0; m < V; ++m) v[m] = src[j + T * m];
+      fft.template run<-1>(v, j, sm, 1);
+      C* out = A.ws + (grp < K::NOUT ? grp : 0) * fs + lo;
+      const bool wr = ok && grp < K::NOUT;
+      r2c_post<F>(v, j, sm, 1, twN, [&](int k, C x) {
+        if (wr) out[k] = x;
+      });
     }
-    if (A.cphys) {
-#pragma unroll
-      for (int c = 0; c < (DIM == 3 ? 3 : 1); ++c) cb[c] = A.cphys[c * A.rs + o];
-      co = cb;
-    }
-    z_pointwise<Tp, DIM, LES, MODEL, PAR2D>(stash, PS, p, uo, co, A.cdx2);
-    if (A.stress_only) {
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) stash[c * PS + p] = (Tp)0;
-    }
-  }
-  __syncthreads();
-  // ---- phase C: r2c of product `grp` (groups >= NOUT run idle for the barriers)
-  {
-    const int gi = grp < K::NOUT ? grp : 0;
-    C v[V];
-    const C* src = reinterpret_cast<const C*>(stash + gi * PS + ln * N);
-#pragma unroll
-    for (int m = 0; m < V; ++m) v[m] = src[j + T * m];
-    fft.template run<-1>(v, j, sm, 1);
-    C* out = A.ws + gi * fs + lo;
-    const bool wr = ok && grp < K::NOUT;
-    r2c_post<F>(v, j, sm, 1, twN, [&](int k, C x) {
-      if (wr) out[k] = x;
-    });
   }
 }
 

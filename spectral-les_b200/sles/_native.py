@@ -23,7 +23,7 @@ EXPORTED = [
     "sles_plan_create", "sles_plan_destroy", "sles_plan_layout", "sles_plan_workspace_bytes",
     "sles_plan_set_workspace", "sles_plan_set_params", "sles_fft_r2c", "sles_fft_c2r",
     "sles_velocity_curl", "sles_velocity_gradient", "sles_rhs", "sles_stage", "sles_diag",
-    "sles_status_string", "sles_version",
+    "sles_status_string", "sles_version", "sles_profile_rhs",
 ]
 
 
@@ -73,6 +73,7 @@ def load_library(path: str = LIB_PATH):
         "sles_stage": (i, [vp, i, d, vp, vp, vp, vp, vp, vp, vp, i, vp]),
         "sles_diag": (i, [vp, vp, vp, vp, vp, i, vp]),
         "sles_status_string": (ctypes.c_char_p, [i]),
+        "sles_profile_rhs": (i, [vp, vp, vp, i, vp, vp]),
         "sles_version": (i, []),
     }
     for name, (res, args) in sig.items():
@@ -158,6 +159,13 @@ class Plan:
     def stage(self, stage, dt, ucur, u0, u1, uout, aux=None, uphys=None, cphys=None, flags=0):
         check(self.L.sles_stage(self.h, int(stage), float(dt), ptr(ucur), ptr(u0), ptr(u1), ptr(uout), ptr(aux),
                                 ptr(uphys), ptr(cphys), int(flags), stream_handle(self.device)), "sles_stage")
+
+    def profile_rhs(self, uh, du, iters):
+        """Mean ms per launch of {x-inverse, y-inverse, z, y-forward, x-forward}."""
+        ms = (ctypes.c_double * 5)()
+        check(self.L.sles_profile_rhs(self.h, ptr(uh), ptr(du), int(iters), ms, stream_handle(self.device)),
+              "sles_profile_rhs")
+        return list(ms)
 
     def diag(self, uh, out, uphys=None, spectrum=None):
         ns = 0 if spectrum is None else spectrum.numel()

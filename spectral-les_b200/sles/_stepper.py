@@ -11,6 +11,10 @@ from __future__ import annotations
 from . import _native as nat
 
 
+# kernels launched by stage() calls since the last reset (counted, not sampled)
+LAUNCHES = [0]
+
+
 def _key(s):
     return (s.data_ptr(), s._version)
 
@@ -19,8 +23,10 @@ def stage(d, k, dt, ucur, u0, u1, uout, aux=None, flags=0, first=False):
     uphys = cphys = None
     if first:
         uphys, cphys = d._phys_override()
-    f = flags | (nat.STAGE_PRIMED if d._primed == _key(ucur) else 0)
+    primed = d._primed == _key(ucur)
+    f = flags | (nat.STAGE_PRIMED if primed else 0)
     d._plan.stage(k, dt, ucur, u0, u1, uout, aux, uphys, cphys, f)
+    LAUNCHES[0] += (4 if d.dim == 3 else 2) + (0 if primed else 1)
     d._primed = None if (flags & nat.STAGE_NO_PREPARE) else _key(uout)
 
 
