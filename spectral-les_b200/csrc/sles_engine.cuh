@@ -3,6 +3,7 @@
 // in parallel; sles_api.cu dispatches to them through the Engine interface.
 #pragma once
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <mutex>
 #include <unordered_map>
 #include <unordered_set>
@@ -106,6 +107,37 @@ inline int launch_persistent(void (*kern)(KArgs...), long long work, int block, 
   return cuda_status(cudaGetLastError());
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+inline PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  return fn;
+}
+
+// 4D tile map over half-complex fields as 8-byte elements:
+// {nk*epc columns, rows, slices, slots}; box {box_cols*epc, box_rows, 1, 1}
+inline int make_tmap(CUtensorMap* m, const void* base, int epc, int nk, long long rows, long long row_stride_b,
+                     long long slices, long long slice_stride_b, long long nslot, long long slot_stride_b,
+                     int box_cols, int box_rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 fn = tmap_encoder();
+  if (!fn) return SLES_ERR_CUDA;
+  cuuint64_t dims[4] = {(cuuint64_t)nk * epc, (cuuint64_t)rows, (cuuint64_t)slices, (cuuint64_t)nslot};
+  cuuint64_t strides[3] = {(cuuint64_t)row_stride_b, (cuuint64_t)slice_stride_b, (cuuint64_t)slot_stride_b};
+  cuuint32_t box[4] = {(cuuint32_t)(box_cols * epc), (cuuint32_t)box_rows, 1, 1};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(base), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? SLES_OK : SLES_ERR_CUDA;
+}
+
 #define SLES_TRY(x)              \
   do {                           \
     int _s = (x);                \
@@ -195,9 +227,7 @@ struct EngineImpl final : Engine {
   using TR = Transforms<Tp, N, DIM>;
   using FX = typename PlanLo<Tp, N>::F;
   using FY = typename PlanLo<Tp, N>::F;
-  static constexpr int W = Cols<Tp>::W;
-  static constexpr int GX = cmax(1, 256 / (W * FX::T));
-  static constexpr int GY = cmax(1, 256 / (W * FY::T));
+  static constexpr int W = XGeo<Tp, N, FX, DIM>::W;
   static constexpr int TZ = PlanFor<Tp, N / 2>::F::T;
   static constexpr int LPI = cmax(1, 16 / TZ);
 
@@ -257,11 +287,32 @@ struct EngineImpl final : Engine {
     return a;
   }
 
+  // x-pass tile map over `nslot` fields starting at base
+  int xmap(const PlanInfo& p, CUtensorMap* m, const void* base, int nslot) const {
+    using K = TGeo<Tp, N, FX>;
+    const long long cb = sizeof(C);
+    if (DIM == 3)
+      return make_tmap(m, base, K::EPC, p.nk, N, (long long)N * p.nkp * cb, N, (long long)p.nkp * cb, nslot,
+                       p.hc_elems * cb, K::W, K::RB);
+    return make_tmap(m, base, K::EPC, p.nk, N, (long long)p.nkp * cb, 1, (long long)N * p.nkp * cb, nslot,
+                     p.hc_elems * cb, K::W, K::RB);
+  }
+
   template <int LES, int PAR2D>
-  int xpass(const PlanInfo& p, const XArgs<Tp>& a, cudaStream_t st) {
-    using K = XGeo<Tp, N, FX, W, GX>;
+  int xpass(const PlanInfo& p, XArgs<Tp> a, cudaStream_t st) {
+    using K = XGeo<Tp, N, FX, DIM>;
+    // state tiles the stage reads (ucur for viscous/forcing/update; u0 when
+    // distinct from ucur; u1 = RK4 accumulator or ETD2's previous F1)
+    a.need_uc = a.need_u0 = a.need_u1 = 0;
+    if (a.fwd && a.kind != KX_RAW) {
+      a.need_uc = 1;
+      const bool uses_u0 = a.kind == KX_RK4 ? a.stage < 3 : (a.kind == KX_RK3P || a.kind == KX_SSP3);
+      a.need_u0 = (uses_u0 && a.u0 != a.ucur) ? 1 : 0;
+      a.need_u1 = (a.kind == KX_RK4 || a.kind == KX_ETD2P || a.kind == KX_ETD2C) ? 1 : 0;
+    }
+    a.err = p.flags;
     const long long items = (long long)(DIM == 3 ? N : 1) * nchunks(p);
-    return launch_persistent(k_xpass<Tp, N, FX, W, GX, DIM, LES, PAR2D>, (items + GX - 1) / GX, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_xpass<Tp, N, FX, DIM, LES, PAR2D>, items, K::THREADS, K::SMEM, st, a);
   }
   int xpass_rt(const PlanInfo& p, const XArgs<Tp>& a, int les, int par2d, cudaStream_t st) {
     if (!les) return xpass<0, 0>(p, a, st);
@@ -272,11 +323,20 @@ struct EngineImpl final : Engine {
   template <int LES>
   int ypass(const PlanInfo& p, int inv, cudaStream_t st) {
     if (DIM != 3) return SLES_OK;
-    using K = XGeo<Tp, N, FY, W, GY>;
-    YArgs<Tp> a{slot(p, 0), p.hc_elems, p.nkp, p.nk, nchunks(p)};
+    using K = TGeo<Tp, N, FY>;
+    YArgs<Tp> a{};
+    const long long cb = sizeof(C);
+    SLES_TRY(make_tmap(&a.tm, slot(p, 0), K::EPC, p.nk, N, (long long)p.nkp * cb, N, (long long)N * p.nkp * cb,
+                       p.ws_fields, p.hc_elems * cb, K::W, K::RB));
+    a.err = p.flags;
+    a.ws = slot(p, 0);
+    a.fs = p.hc_elems;
+    a.nkp = p.nkp;
+    a.nk = p.nk;
+    a.nchunks = nchunks(p);
     const long long items = (long long)N * nchunks(p);
-    if (inv) return launch_persistent(k_ypass_inv<Tp, N, FY, W, GY, LES>, (items + GY - 1) / GY, K::THREADS, K::SMEM, st, a);
-    return launch_persistent(k_ypass_fwd<Tp, N, FY, W, GY, LES>, (items + GY - 1) / GY, K::THREADS, K::SMEM, st, a);
+    if (inv) return launch_persistent(k_ypass<Tp, N, FY, LES, 1>, items, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_ypass<Tp, N, FY, LES, 0>, items, K::THREADS, K::SMEM, st, a);
   }
 
   template <int LES, int MODEL, int PAR2D>

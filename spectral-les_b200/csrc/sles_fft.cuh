@@ -219,6 +219,59 @@ struct LineFFT {
     }
   }
 
+  // Same stage with twiddles read from a shared table tab[e] = exp(-2 pi i e/L)
+  // (threads of one line share j, so a warp reads few distinct entries).
+  template <int R, int DIR, bool LAST>
+  __device__ __forceinline__ void stage_tab(C (&v)[V], const C* tab, int Ns, int j, C* sm, int ws) {
+    constexpr int NB = (L / R) / T;
+    const int stride = L / (Ns * R);
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+      C u[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) u[r] = v[q + r * NB];
+      const int b = j + T * q;
+      const int k = b % Ns;
+      if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const C w = tab[k * r * stride];
+          u[r] = (DIR < 0) ? cmul(u[r], w) : cmulc(u[r], w);
+        }
+      }
+      dft<R, DIR>(u);
+      if constexpr (LAST) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[q + r * NB] = u[r];
+      } else {
+        const int idxD = (b / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) sm[xpad(idxD + r * Ns) * ws] = u[r];
+      }
+    }
+  }
+
+  // Transform with twiddles from `tab` (L entries, see fill_table); needs no init().
+  template <int DIR>
+  __device__ __forceinline__ void run_tab(C (&v)[V], int j, C* sm, int ws, const C* tab) {
+    if constexpr (S >= 2) __syncthreads();
+    stage_tab<R0, DIR, S == 1>(v, tab, 1, j, sm, ws);
+    if constexpr (S >= 2) {
+      exchange(v, j, sm, ws);
+      if constexpr (S >= 3) __syncthreads();
+      stage_tab<R1, DIR, S == 2>(v, tab, R0, j, sm, ws);
+    }
+    if constexpr (S >= 3) {
+      exchange(v, j, sm, ws);
+      stage_tab<R2, DIR, true>(v, tab, R0 * R1, j, sm, ws);
+    }
+  }
+
+  // cooperative fill of the twiddle table (float64, rounded once)
+  __device__ __forceinline__ static void fill_table(C* tab) {
+    for (int e = threadIdx.x; e < L; e += blockDim.x) tab[e] = twiddle<Tp>(e, L, -1);
+  }
+
   __device__ __forceinline__ void exchange(C (&v)[V], int j, C* sm, int ws) {
     __syncthreads();
 #pragma unroll

@@ -37,6 +37,7 @@
 // calculate_nuR, src/smagorinsky.py:24-47 and src/vreman.py:30-147.
 #pragma once
 #include "sles_passes.cuh"
+#include "sles_tma.cuh"
 
 namespace sles {
 
@@ -46,6 +47,8 @@ enum LesModel { M_NONE = 0, M_SMAG = 1, M_VREMAN = 2 };
 template <typename Tp>
 struct XArgs {
   using C = typename CT<Tp>::C;
+  int need_uc, need_u0, need_u1;  // which state fields the stage reads (u0 aliasing ucur: need_u0 = 0)
+  unsigned* err;
   C* ws;                 // workspace slot 0
   long long fs;          // elements per half-complex field
   int nkp, nk, nchunks;
@@ -65,14 +68,12 @@ struct XArgs {
   double nu_d, dt_d;     // ETD2 weights are evaluated in float64
 };
 
-// Per-position spectral combine and stage update for D velocity components.
-// S[c] holds R_c (nonlinear + stress term before masking) on entry and the
-// new state (or dU) on exit.  k[c]: integer wavenumbers; off: element offset.
+// Per-position mask and projection for D velocity components (in place):
+// R <- mask * R, then R <- R - k (k . R)/|k|^2 (src/RK4_method.py:48-57);
+// KX_RAW keeps the masked term unprojected (the LES stress T_hat alone).
 template <typename Tp, int D>
-__device__ __forceinline__ void combine_update(const XArgs<Tp>& A, typename CT<Tp>::C (&S)[D], const int (&k)[D],
-                                               long long off) {
+__device__ __forceinline__ void project(const XArgs<Tp>& A, typename CT<Tp>::C (&R)[D], const int (&k)[D]) {
   using C = typename CT<Tp>::C;
-  const long long fs = A.fs;
   int k2 = 0;
   bool in = true;
 #pragma unroll
@@ -81,35 +82,33 @@ __device__ __forceinline__ void combine_update(const XArgs<Tp>& A, typename CT<T
     in = in && fabs((double)k[c]) < A.kmax;  // initialize_domain.py:109-114
   }
   const double kk = (double)(k2 == 0 ? 1 : k2);  // K_over_K2, initialize_domain.py:163-165
-  C R[D], Uc[D];
   C P = cmk<C>(0, 0);
 #pragma unroll
   for (int c = 0; c < D; ++c) {
-    R[c] = in ? S[c] : cmk<C>(0, 0);  // dU *= dealias (RK4_method.py:48)
+    R[c] = in ? R[c] : cmk<C>(0, 0);
     P = cadd(P, cscale(R[c], (Tp)((double)k[c] / kk)));
   }
-  if (A.kind == KX_RAW) {  // masked term only (the LES stress T_hat)
+  if (A.kind == KX_RAW) return;
 #pragma unroll
-    for (int c = 0; c < D; ++c) {
-      A.uout[c * fs + off] = R[c];
-      S[c] = R[c];
-    }
-    return;
+  for (int c = 0; c < D; ++c) R[c] = csub(R[c], cscale(P, (Tp)k[c]));
+}
+
+// Stage update of one component at one position.  R: projected term of
+// component c; uc/u0/u1: state values at this position (u1: RK4 accumulator
+// or ETD2's previous F1).  Writes uout/u1/aux and returns the new state.
+template <typename Tp>
+__device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& A, int c, typename CT<Tp>::C R,
+                                                              typename CT<Tp>::C uc, typename CT<Tp>::C u0,
+                                                              typename CT<Tp>::C u1, int k2, long long off) {
+  using C = typename CT<Tp>::C;
+  const long long o = c * A.fs + off;
+  if (A.kind == KX_RAW) {
+    A.uout[o] = R;
+    return R;
   }
-#pragma unroll
-  for (int c = 0; c < D; ++c) {
-    R[c] = csub(R[c], cscale(P, (Tp)k[c]));  // RK4_method.py:52-57
-    Uc[c] = A.ucur[c * fs + off];
-  }
-  if (A.forcing > (Tp)0 && k2 != 0) {  // RK4_method.py:58-64
-#pragma unroll
-    for (int c = 0; c < D; ++c) R[c] = cadd(R[c], cscale(Uc[c], A.forcing));
-  }
-  if (A.record_f1) {  // RK4_method.py:65-66
-#pragma unroll
-    for (int c = 0; c < D; ++c)
-      A.aux[c * fs + off] = (A.record_f1 == 2) ? csub(R[c], A.aux[c * fs + off]) : R[c];
-  }
+  if (A.forcing > (Tp)0 && k2 != 0) R = cadd(R, cscale(uc, A.forcing));  // RK4_method.py:58-64
+  if (A.record_f1) A.aux[o] = (A.record_f1 == 2) ? csub(R, A.aux[o]) : R;  // RK4_method.py:65-66
+  C un;
   if (A.kind == KX_ETD2P || A.kind == KX_ETD2C) {
     // parity: src/ETD2_method.py:16-29; corrected: Cox & Matthews (2002) eq. 22
     const double z = A.dt_d * A.nu_d * (double)k2;
@@ -129,100 +128,141 @@ __device__ __forceinline__ void combine_update(const XArgs<Tp>& A, typename CT<T
       w1 = h * ((1.0 - z) * E - 1.0 + 2.0 * z) / (z * z);
       w0 = h * (-E + 1.0 - z) / (z * z);
     }
-#pragma unroll
-    for (int c = 0; c < D; ++c) {
-      const C F0 = A.u1[c * fs + off];
-      const C un = cadd(cscale(Uc[c], (Tp)E), cadd(cscale(R[c], (Tp)w1), cscale(F0, (Tp)w0)));
-      A.aux[c * fs + off] = R[c];
-      A.uout[c * fs + off] = un;
-      S[c] = un;
-    }
-    return;
-  }
-  const Tp nk2 = A.nu * (Tp)k2;  // (nu * K2) * U_hat, RK4_method.py:67-68
-#pragma unroll
-  for (int c = 0; c < D; ++c) {
-    const C dU = csub(R[c], cscale(Uc[c], nk2));
-    const long long o = c * fs + off;
-    C un;
-    switch (A.kind) {
-      case KX_RK4:  // RK4_method.py:20-27
-        if (A.stage < 3) {
-          A.u1[o] = cadd(A.u1[o], cscale(dU, A.c1));
-          un = cadd(A.u0[o], cscale(dU, A.c2));
-        } else {
-          un = cadd(A.u1[o], cscale(dU, A.c1));
-          A.u1[o] = un;
-        }
-        break;
-      case KX_RK3P:  // RK3_method.py:26-33
-        if (A.stage == 0) {
-          un = cadd(A.u0[o], cscale(dU, A.c2));
-        } else if (A.stage == 1) {
-          un = cadd(csub(A.u0[o], cscale(dU, A.c1)), cscale(dU, A.c2));
-        } else {
-          const C t = cadd(cadd(cscale(dU, (Tp)(1.0 / 6.0)), cscale(dU, (Tp)(2.0 / 3.0))), cscale(dU, (Tp)(1.0 / 6.0)));
-          un = cadd(A.u0[o], cscale(t, A.c1));
-        }
-        break;
-      case KX_SSP3:  // Shu & Osher (1988)
-        if (A.stage == 0) {
-          un = cadd(A.u0[o], cscale(dU, A.c1));
-        } else if (A.stage == 1) {
-          un = cadd(cscale(A.u0[o], (Tp)0.75), cscale(cadd(Uc[c], cscale(dU, A.c1)), (Tp)0.25));
-        } else {
-          un = cadd(cscale(A.u0[o], (Tp)(1.0 / 3.0)), cscale(cadd(Uc[c], cscale(dU, A.c1)), (Tp)(2.0 / 3.0)));
-        }
-        break;
-      default:  // KX_RHS
-        un = dU;
-        break;
-    }
+    un = cadd(cscale(uc, (Tp)E), cadd(cscale(R, (Tp)w1), cscale(u1, (Tp)w0)));
+    A.aux[o] = R;
     A.uout[o] = un;
-    S[c] = un;
+    return un;
   }
+  const C dU = csub(R, cscale(uc, A.nu * (Tp)k2));  // (nu * K2) * U_hat, RK4_method.py:67-68
+  switch (A.kind) {
+    case KX_RK4:  // RK4_method.py:20-27
+      if (A.stage < 3) {
+        A.u1[o] = cadd(u1, cscale(dU, A.c1));
+        un = cadd(u0, cscale(dU, A.c2));
+      } else {
+        un = cadd(u1, cscale(dU, A.c1));
+        A.u1[o] = un;
+      }
+      break;
+    case KX_RK3P:  // RK3_method.py:26-33
+      if (A.stage == 0) {
+        un = cadd(u0, cscale(dU, A.c2));
+      } else if (A.stage == 1) {
+        un = cadd(csub(u0, cscale(dU, A.c1)), cscale(dU, A.c2));
+      } else {
+        const C t = cadd(cadd(cscale(dU, (Tp)(1.0 / 6.0)), cscale(dU, (Tp)(2.0 / 3.0))), cscale(dU, (Tp)(1.0 / 6.0)));
+        un = cadd(u0, cscale(t, A.c1));
+      }
+      break;
+    case KX_SSP3:  // Shu & Osher (1988)
+      if (A.stage == 0) {
+        un = cadd(u0, cscale(dU, A.c1));
+      } else if (A.stage == 1) {
+        un = cadd(cscale(u0, (Tp)0.75), cscale(cadd(uc, cscale(dU, A.c1)), (Tp)0.25));
+      } else {
+        un = cadd(cscale(u0, (Tp)(1.0 / 3.0)), cscale(cadd(uc, cscale(dU, A.c1)), (Tp)(2.0 / 3.0)));
+      }
+      break;
+    default:  // KX_RHS
+      un = dU;
+      break;
+  }
+  A.uout[o] = un;
+  return un;
+}
+
+// ---------------------------------------------------------------------------
+// Strided-axis pass geometry: one work item (W lines of N points) per block
+// iteration; tiles arrive by TMA into a ring of NBUF buffers.
+// ---------------------------------------------------------------------------
+template <typename Tp, int N, class F, bool RING = true, int NBUF_SET = 0>
+struct TGeo {
+  using C = typename CT<Tp>::C;
+  static constexpr int W = (sizeof(Tp) == 4) ? 8 : 4;       // 64-byte tile rows
+  static constexpr int EPC = sizeof(C) / 8;                 // 8-byte tensor elements per complex
+  static constexpr int T = F::T, V = F::V;
+  static constexpr int THREADS = W * T;
+  static constexpr int RB = N < 256 ? N : 256;              // rows per TMA box
+  static constexpr int NBOX = N / RB;
+  static constexpr int TE = N * W;                          // complex elements per tile
+  static constexpr int NBUF =
+      NBUF_SET > 0 ? NBUF_SET : ((TE * sizeof(C) <= 16384) ? 4 : ((TE * sizeof(C) <= 32768) ? 3 : 2));
+  static constexpr unsigned BOX_BYTES = RB * W * sizeof(C);
+  static constexpr int SCR = xline_len(N) * W;
+  using Ring = TileRing<C, NBUF, TE>;
+  static constexpr size_t RING_BYTES = RING ? Ring::bytes() : 0;
+  static constexpr size_t SMEM = RING_BYTES + ((size_t)SCR + N) * sizeof(C);  // + twiddle table
+#ifndef SLES_T_MINB256
+#define SLES_T_MINB256 2
+#endif
+  static constexpr int MINB = (sizeof(Tp) == 4) ? (THREADS >= 512 ? 1 : (THREADS >= 256 ? SLES_T_MINB256 : 4)) : 1;
+};
+
+// x-pass geometry: direct coalesced loads, the projected components kept in
+// a shared stash [D][N][W] between the forward and the per-component phase
+template <typename Tp, int N, class F, int DIM>
+struct XGeo {
+  using C = typename CT<Tp>::C;
+  static constexpr int W = (sizeof(Tp) == 4) ? 8 : 4;
+  static constexpr int T = F::T, V = F::V;
+  static constexpr int THREADS = W * T;
+  static constexpr int TE = N * W;
+  static constexpr int SCR = xline_len(N) * W;
+  static constexpr size_t SMEM = ((size_t)DIM * TE + SCR + N) * sizeof(C);
+#ifndef SLES_X_MINB256
+#define SLES_X_MINB256 2
+#endif
+  static constexpr int MINB = (sizeof(Tp) == 4) ? (THREADS >= 512 ? 1 : (THREADS >= 256 ? SLES_X_MINB256 : 4)) : 1;
+};
+
+// slot of tile `i` in a pass's per-item load sequence
+template <int KIND>
+__device__ __forceinline__ int seq_slot(int i) {
+  // 0: y-inverse LES, 1: y-inverse plain, 2: y-forward LES, 3: y-forward plain / x plain 3D,
+  // 4: x LES 3D, 5: identity (x 2D, inverse-only sources)
+  if (KIND == 0) { const int s[6] = {0, 3, 1, 4, 2, 5}; return s[i]; }
+  if (KIND == 1) { const int s[5] = {2, 0, 4, 1, 3}; return s[i]; }
+  if (KIND == 2) { const int s[9] = {4, 5, 0, 3, 6, 7, 1, 8, 2}; return s[i]; }
+  if (KIND == 4) { const int s[6] = {0, 3, 1, 4, 2, 5}; return s[i]; }
+  return i;
 }
 
 // ---------------------------------------------------------------------------
 // X pass.  Work item = (ky slice [3D], column chunk of W last-axis wavenumbers);
 // lines along x.  PAR2D selects the reference's 2D stress (1) or the corrected one.
 // ---------------------------------------------------------------------------
-template <typename Tp, int N, class F, int W, int G>
-struct XGeo {
-  static constexpr int T = F::T, V = F::V, THREADS = G * W * T, SCR = xline_len(N) * W;
-  // resident blocks per SM the register allocation must allow
-  static constexpr int MINB = (THREADS >= 512) ? 1 : (sizeof(Tp) == 4 ? 2 : 1);
-  static constexpr size_t SMEM = (size_t)G * SCR * sizeof(typename CT<Tp>::C);
-};
-
-template <typename Tp, int N, class F, int W, int G, int DIM, int LES, int PAR2D>
-__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS, XGeo<Tp, N, F, W, G>::MINB) k_xpass(const XArgs<Tp> A) {
-  using K = XGeo<Tp, N, F, W, G>;
+template <typename Tp, int N, class F, int DIM, int LES, int PAR2D>
+__global__ void __launch_bounds__(XGeo<Tp, N, F, DIM>::THREADS, XGeo<Tp, N, F, DIM>::MINB)
+k_xpass(const __grid_constant__ XArgs<Tp> A) {
+  using K = XGeo<Tp, N, F, DIM>;
   using C = typename CT<Tp>::C;
-  constexpr int T = K::T, V = K::V, D = DIM;
+  constexpr int T = K::T, V = K::V, D = DIM, W = K::W;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* scr = reinterpret_cast<C*>(smem_raw);
+  C* rst = reinterpret_cast<C*>(smem_raw);  // [D][N][W] projected components
+  C* sm0 = rst + D * K::TE;                 // exchange scratch
+  C* twt = sm0 + K::SCR;                    // twiddle table exp(-2 pi i e/N)
   const int tid = threadIdx.x;
-  const int l = tid % W, j = (tid / W) % T, g = tid / (W * T);
+  const int l = tid % W, j = tid / W;
+  F::fill_table(twt);
+  __syncthreads();
   F fft;
-  fft.init(j);
-  const long long items_ = (long long)((DIM == 3) ? N : 1) * A.nchunks;
-  const long long nbi_ = (items_ + G - 1) / G;
-  for (long long bi = blockIdx.x; bi < nbi_; bi += gridDim.x) {  // persistent over work items
-    const long long it = bi * G + g;
+  const int nsl = (DIM == 3) ? N : 1;
+  const long long items = (long long)nsl * A.nchunks;
+  const long long ps = (DIM == 3) ? (long long)N * A.nkp : (long long)A.nkp;
+  const long long fs = A.fs;
+  C* sm = sm0 + l;
+  C* ws = A.ws;
+  auto kx_at = [&](int m) { return kc2c(j + T * m, N); };
+  auto rpos = [&](int c, int m) { return c * K::TE + (j + T * m) * W + l; };
+  for (long long it = blockIdx.x; it < items; it += gridDim.x) {  // persistent over work items
     const int chunk = (int)(it % A.nchunks);
-    const int sl = (int)(it / A.nchunks);            // ky slice (3D); 0 in 2D
-    const int nsl = (DIM == 3) ? N : 1;
+    const int sl = (int)(it / A.nchunks);  // ky slice (3D); 0 in 2D
     const int col = chunk * W + l;
-    const bool ok = sl < nsl && col < A.nk;
-    const long long base = (long long)(sl < nsl ? sl : 0) * A.nkp + col;
-    const long long ps = (DIM == 3) ? (long long)N * A.nkp : (long long)A.nkp;
-    const long long fs = A.fs;
-    C* sm = scr + g * K::SCR + l;
-    C* ws = A.ws;
-    auto ld = [&](const C* f, C (&v)[V]) {
+    const bool ok = col < A.nk;
+    const long long base = (long long)sl * A.nkp + col;
+    auto ld = [&](C (&v)[V], const C* src, int slot) {
 #pragma unroll
-      for (int m = 0; m < V; ++m) v[m] = ok ? f[base + (j + T * m) * ps] : cmk<C>(0, 0);
+      for (int m = 0; m < V; ++m) v[m] = ok ? src[slot * fs + base + (j + T * m) * ps] : cmk<C>(0, 0);
     };
     auto st = [&](int slot, const C (&v)[V]) {
       if (ok) {
@@ -230,110 +270,108 @@ __global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS, XGeo<Tp, N, F, 
         for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
       }
     };
-    auto kx_at = [&](int m) { return kc2c(j + T * m, N); };
-    C S[D][V];
-    if (A.fwd) {
-      if (DIM == 3) {
+    // inverse x-transforms of component c of the new state: primes the next evaluation
+    auto prep = [&](int c, C (&s)[V]) {
+      if (LES) {
+        C b[V];
 #pragma unroll
-        for (int c = 0; c < D; ++c) {
-          ld(ws + c * fs, S[c]);
-          fft.template run<-1>(S[c], j, sm, W);
-          if (LES) {  // + 2i kx F_cx
-            C h[V];
-            ld(ws + (3 + c) * fs, h);
-            fft.template run<-1>(h, j, sm, W);
+        for (int m = 0; m < V; ++m) b[m] = cmuli_s(s[m], (Tp)kx_at(m));  // i kx u_c
+        fft.template run_tab<+1>(b, j, sm, W, twt);
+        st(D + c, b);
+      } else if ((DIM == 3 && c >= 1) || (DIM == 2 && c == 1)) {
+        C q[V];
+        const Tp sg = (DIM == 3 && c == 2) ? (Tp)-1 : (Tp)1;  // 3D: -i kx w -> [3], i kx v -> [4]; 2D: i kx v -> [2]
 #pragma unroll
-            for (int m = 0; m < V; ++m) S[c][m] = cadd(S[c][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
-          }
-        }
-      } else {
-        const Tp ky2 = (Tp)(2 * col);
-#pragma unroll
-        for (int c = 0; c < D; ++c) {
-          ld(ws + c * fs, S[c]);
-          fft.template run<-1>(S[c], j, sm, W);
-        }
-        if (LES) {
-          // reference (math_formula.py:128-146): T_0 = 2i(kx F12 + ky F22), T_1 = 0
-          // corrected: T_0 = 2i(kx F11 + ky F12), T_1 = 2i(kx F12 + ky F22)
-          C h[V];
-          ld(ws + 2 * fs, h);
-          fft.template run<-1>(h, j, sm, W);
-#pragma unroll
-          for (int m = 0; m < V; ++m) S[0][m] = cadd(S[0][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
-          ld(ws + 3 * fs, h);
-          fft.template run<-1>(h, j, sm, W);
-#pragma unroll
-          for (int m = 0; m < V; ++m) {
-            S[0][m] = cadd(S[0][m], cmuli_s(h[m], ky2));
-            if (!PAR2D) S[1][m] = cadd(S[1][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
-          }
-          if (!PAR2D) {
-            ld(ws + 4 * fs, h);
-            fft.template run<-1>(h, j, sm, W);
-#pragma unroll
-            for (int m = 0; m < V; ++m) S[1][m] = cadd(S[1][m], cmuli_s(h[m], ky2));
-          }
-        }
+        for (int m = 0; m < V; ++m) q[m] = cmuli_s(s[m], sg * (Tp)kx_at(m));
+        fft.template run_tab<+1>(q, j, sm, W, twt);
+        st(DIM == 3 ? (c == 2 ? 3 : 4) : 2, q);
       }
+      fft.template run_tab<+1>(s, j, sm, W, twt);
+      st(c, s);
+    };
+    if (!A.fwd) {
+#pragma unroll 1
+      for (int c = 0; c < D; ++c) {
+        C v[V];
+        ld(v, A.uinv, c);
+        prep(c, v);
+      }
+      continue;
+    }
+    // forward x-transforms; the x part of div(tau) joins in spectral space
+#pragma unroll 1
+    for (int c = 0; c < D; ++c) {
+      C v[V];
+      ld(v, ws, c);
+      fft.template run_tab<-1>(v, j, sm, W, twt);
+      if (LES && DIM == 3) {  // + 2i kx F_cx
+        C h[V];
+        ld(h, ws, 3 + c);
+        fft.template run_tab<-1>(h, j, sm, W, twt);
+#pragma unroll
+        for (int m = 0; m < V; ++m) v[m] = cadd(v[m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+      }
+#pragma unroll
+      for (int m = 0; m < V; ++m) rst[rpos(c, m)] = v[m];
+    }
+    if (LES && DIM == 2) {
+      // reference (math_formula.py:128-146): T_0 = 2i(kx F12 + ky F22), T_1 = 0
+      // corrected: T_0 = 2i(kx F11 + ky F12), T_1 = 2i(kx F12 + ky F22)
+      const Tp ky2 = (Tp)(2 * col);
+      C h[V];
+      ld(h, ws, 2);
+      fft.template run_tab<-1>(h, j, sm, W, twt);
+#pragma unroll
+      for (int m = 0; m < V; ++m) rst[rpos(0, m)] = cadd(rst[rpos(0, m)], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+      ld(h, ws, 3);
+      fft.template run_tab<-1>(h, j, sm, W, twt);
+#pragma unroll
+      for (int m = 0; m < V; ++m) {
+        rst[rpos(0, m)] = cadd(rst[rpos(0, m)], cmuli_s(h[m], ky2));
+        if (!PAR2D) rst[rpos(1, m)] = cadd(rst[rpos(1, m)], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+      }
+      if (!PAR2D) {
+        ld(h, ws, 4);
+        fft.template run_tab<-1>(h, j, sm, W, twt);
+#pragma unroll
+        for (int m = 0; m < V; ++m) rst[rpos(1, m)] = cadd(rst[rpos(1, m)], cmuli_s(h[m], ky2));
+      }
+    }
+    // mask + projection (each thread revisits only its own stash positions)
+#pragma unroll
+    for (int m = 0; m < V; ++m) {
+      C s[D];
+      int kv[D];
+#pragma unroll
+      for (int c = 0; c < D; ++c) s[c] = rst[rpos(c, m)];
+      kv[0] = kx_at(m);
+      if (DIM == 3) { kv[1] = kc2c(sl, N); kv[D - 1] = col; }
+      else kv[1] = col;
+      project<Tp, D>(A, s, kv);
+#pragma unroll
+      for (int c = 0; c < D; ++c) rst[rpos(c, m)] = s[c];
+    }
+    // per component: state update, then the inverse transforms of the new state
+    const int kyv = (DIM == 3) ? kc2c(sl, N) : 0;
+#pragma unroll 1
+    for (int c = 0; c < D; ++c) {
+      C v[V];
       if (ok) {
 #pragma unroll
         for (int m = 0; m < V; ++m) {
-          C s[D];
-          int k[D];
-#pragma unroll
-          for (int c = 0; c < D; ++c) s[c] = S[c][m];
-          k[0] = kx_at(m);
-          if (DIM == 3) { k[1] = kc2c(sl, N); k[D - 1] = col; }
-          else k[1] = col;
-          combine_update<Tp, D>(A, s, k, base + (j + T * m) * ps);
-#pragma unroll
-          for (int c = 0; c < D; ++c) S[c][m] = s[c];
-        }
-      }
-    } else {
-#pragma unroll
-      for (int c = 0; c < D; ++c) ld(A.uinv + c * fs, S[c]);
-    }
-    if (A.prep) {  // uniform across the block
-      if (LES) {
-#pragma unroll
-        for (int c = 0; c < D; ++c) {
-          C b[V];
-#pragma unroll
-          for (int m = 0; m < V; ++m) b[m] = cmuli_s(S[c][m], (Tp)kx_at(m));
-          fft.template run<+1>(b, j, sm, W);
-          st(D + c, b);
-          fft.template run<+1>(S[c], j, sm, W);
-          st(c, S[c]);
-        }
-      } else if (DIM == 3) {
-        C q[V];
-#pragma unroll
-        for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[2][m], -(Tp)kx_at(m));  // -i kx w
-        fft.template run<+1>(q, j, sm, W);
-        st(3, q);
-#pragma unroll
-        for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[1][m], (Tp)kx_at(m));   //  i kx v
-        fft.template run<+1>(q, j, sm, W);
-        st(4, q);
-#pragma unroll
-        for (int c = 0; c < D; ++c) {
-          fft.template run<+1>(S[c], j, sm, W);
-          st(c, S[c]);
+          const long long off = base + (j + T * m) * ps;
+          const int kx = kx_at(m);
+          const int k2 = kx * kx + kyv * kyv + col * col;
+          const C ucm = A.need_uc ? A.ucur[c * fs + off] : cmk<C>(0, 0);
+          const C u0m = A.need_u0 ? A.u0[c * fs + off] : ucm;
+          const C u1m = A.need_u1 ? A.u1[c * fs + off] : cmk<C>(0, 0);
+          v[m] = update_component<Tp>(A, c, rst[rpos(c, m)], ucm, u0m, u1m, k2, off);
         }
       } else {
-        C q[V];
 #pragma unroll
-        for (int m = 0; m < V; ++m) q[m] = cmuli_s(S[1][m], (Tp)kx_at(m));   //  i kx v
-        fft.template run<+1>(q, j, sm, W);
-        st(2, q);
-#pragma unroll
-        for (int c = 0; c < D; ++c) {
-          fft.template run<+1>(S[c], j, sm, W);
-          st(c, S[c]);
-        }
+        for (int m = 0; m < V; ++m) v[m] = cmk<C>(0, 0);
       }
+      if (A.prep) prep(c, v);
     }
   }
 }
@@ -344,178 +382,169 @@ __global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS, XGeo<Tp, N, F, 
 template <typename Tp>
 struct YArgs {
   using C = typename CT<Tp>::C;
+  CUtensorMap tm;        // workspace slots as y-pass tiles
+  unsigned* err;
   C* ws;
   long long fs;
   int nkp, nk, nchunks;
 };
 
-template <typename Tp, int N, class F, int W, int G, int LES>
-__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS, XGeo<Tp, N, F, W, G>::MINB) k_ypass_inv(const YArgs<Tp> A) {
-  using K = XGeo<Tp, N, F, W, G>;
+// INV = 1: inverse (y1), 0: forward (y2)
+template <typename Tp, int N, class F, int LES, int INV>
+__global__ void __launch_bounds__(TGeo<Tp, N, F>::THREADS, TGeo<Tp, N, F>::MINB)
+k_ypass(const __grid_constant__ YArgs<Tp> A) {
+  using K = TGeo<Tp, N, F>;
   using C = typename CT<Tp>::C;
-  constexpr int T = K::T, V = K::V;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* scr = reinterpret_cast<C*>(smem_raw);
+  constexpr int T = K::T, V = K::V, W = K::W;
+  constexpr int KIND = INV ? (LES ? 0 : 1) : (LES ? 2 : 3);
+  constexpr int NT = INV ? (LES ? 6 : 5) : (LES ? 9 : 3);
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  typename K::Ring ring;
   const int tid = threadIdx.x;
-  const int l = tid % W, j = (tid / W) % T, g = tid / (W * T);
+  ring.init(smem_raw, tid);
+  C* sm0 = reinterpret_cast<C*>(smem_raw + K::Ring::bytes());
+  C* twt = sm0 + K::SCR;  // twiddle table exp(-2 pi i e/N)
+  const int l = tid % W, j = tid / W;
   F fft;
-  fft.init(j);
-  const long long items_ = (long long)N * A.nchunks;
-  const long long nbi_ = (items_ + G - 1) / G;
-  for (long long bi = blockIdx.x; bi < nbi_; bi += gridDim.x) {  // persistent over work items
-    const long long it = bi * G + g;
-    const int chunk = (int)(it % A.nchunks);
-    const int x = (int)(it / A.nchunks);
-    const int col = chunk * W + l;
-    const bool ok = x < N && col < A.nk;
-    const long long base = (long long)(x < N ? x : 0) * N * A.nkp + col;
-    const long long ps = A.nkp, fs = A.fs;
-    C* sm = scr + g * K::SCR + l;
-    C* ws = A.ws;
-    auto ld = [&](int slot, C (&v)[V]) {
-#pragma unroll
-      for (int m = 0; m < V; ++m) v[m] = ok ? ws[slot * fs + base + (j + T * m) * ps] : cmk<C>(0, 0);
-    };
-    auto st = [&](int slot, const C (&v)[V]) {
-      if (ok) {
-#pragma unroll
-        for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
-      }
-    };
-    auto iky = [&](const C (&v)[V], C (&w)[V]) {
-#pragma unroll
-      for (int m = 0; m < V; ++m) w[m] = cmuli_s(v[m], (Tp)kc2c(j + T * m, N));
-    };
-    C v[V], w[V];
-    if (LES) {
-#pragma unroll 1
-      for (int c = 0; c < 3; ++c) {
-        ld(c, v);
-        iky(v, w);
-        fft.template run<+1>(v, j, sm, W);
-        st(c, v);
-        fft.template run<+1>(w, j, sm, W);
-        st(6 + c, w);
-        ld(3 + c, v);
-        fft.template run<+1>(v, j, sm, W);
-        st(3 + c, v);
-      }
-    } else {
-      ld(2, v);  // A_w -> a_w and Ox = Y^-1(i ky A_w)
-      iky(v, w);
-      fft.template run<+1>(v, j, sm, W);
-      st(2, v);
-      fft.template run<+1>(w, j, sm, W);
-      st(5, w);
-      ld(0, v);  // A_u -> a_u and Oz = Y^-1(Q_z - i ky A_u)
-      ld(4, w);
-#pragma unroll
-      for (int m = 0; m < V; ++m) w[m] = csub(w[m], cmuli_s(v[m], (Tp)kc2c(j + T * m, N)));
-      fft.template run<+1>(v, j, sm, W);
-      st(0, v);
-      fft.template run<+1>(w, j, sm, W);
-      st(4, w);
-      ld(1, v);
-      fft.template run<+1>(v, j, sm, W);
-      st(1, v);
-      ld(3, v);
-      fft.template run<+1>(v, j, sm, W);
-      st(3, v);
-    }
+  F::fill_table(twt);
+  __syncthreads();
+  const long long items = (long long)N * A.nchunks;
+  const long long mine = (blockIdx.x < items) ? (items - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  const long long ntiles = mine * NT;
+  auto issue = [&](long long t) {
+    const long long it = blockIdx.x + (t / NT) * (long long)gridDim.x;
+    const int chunk = (int)(it % A.nchunks), x = (int)(it / A.nchunks);
+    ring.issue(t, &A.tm, chunk * W * K::EPC, x, seq_slot<KIND>((int)(t % NT)), K::NBOX, K::RB, K::BOX_BYTES);
+  };
+  if (tid == 0) {
+    tma_prefetch_desc(&A.tm);
+    for (long long t = 0; t < K::NBUF && t < ntiles; ++t) issue(t);
   }
-}
-
-template <typename Tp, int N, class F, int W, int G, int LES>
-__global__ void __launch_bounds__(XGeo<Tp, N, F, W, G>::THREADS, XGeo<Tp, N, F, W, G>::MINB) k_ypass_fwd(const YArgs<Tp> A) {
-  using K = XGeo<Tp, N, F, W, G>;
-  using C = typename CT<Tp>::C;
-  constexpr int T = K::T, V = K::V;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* scr = reinterpret_cast<C*>(smem_raw);
-  const int tid = threadIdx.x;
-  const int l = tid % W, j = (tid / W) % T, g = tid / (W * T);
-  F fft;
-  fft.init(j);
-  const long long items_ = (long long)N * A.nchunks;
-  const long long nbi_ = (items_ + G - 1) / G;
-  for (long long bi = blockIdx.x; bi < nbi_; bi += gridDim.x) {  // persistent over work items
-    const long long it = bi * G + g;
+  long long t = 0;
+  auto take = [&](C (&v)[V]) {
+    ring.wait(t, A.err);
+    const C* tl = ring.tile(t);
+#pragma unroll
+    for (int m = 0; m < V; ++m) v[m] = tl[(j + T * m) * W + l];
+    __syncthreads();
+    if (tid == 0 && t + K::NBUF < ntiles) issue(t + K::NBUF);
+    ++t;
+  };
+  const long long ps = A.nkp, fs = A.fs;
+  C* sm = sm0 + l;
+  C* ws = A.ws;
+  auto kyv = [&](int m) { return (Tp)kc2c(j + T * m, N); };
+  for (long long k = 0; k < mine; ++k) {  // persistent over work items
+    const long long it = blockIdx.x + k * (long long)gridDim.x;
     const int chunk = (int)(it % A.nchunks);
     const int x = (int)(it / A.nchunks);
     const int col = chunk * W + l;
-    const bool ok = x < N && col < A.nk;
-    const long long base = (long long)(x < N ? x : 0) * N * A.nkp + col;
-    const long long ps = A.nkp, fs = A.fs;
-    C* sm = scr + g * K::SCR + l;
-    C* ws = A.ws;
-    auto ld = [&](int slot, C (&v)[V]) {
-#pragma unroll
-      for (int m = 0; m < V; ++m) v[m] = ok ? ws[slot * fs + base + (j + T * m) * ps] : cmk<C>(0, 0);
-    };
+    const bool ok = col < A.nk;
+    const long long base = (long long)x * N * A.nkp + col;
     auto st = [&](int slot, const C (&v)[V]) {
       if (ok) {
 #pragma unroll
         for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
       }
     };
+    if (INV) {
+      C v[V], w[V];
+      if (LES) {
+#pragma unroll 1
+        for (int c = 0; c < 3; ++c) {  // a_c, dy_c = Y^-1(i ky A_c), dx_c = Y^-1(B_c)
+          take(v);
+#pragma unroll
+          for (int m = 0; m < V; ++m) w[m] = cmuli_s(v[m], kyv(m));
+          fft.template run_tab<+1>(v, j, sm, W, twt);
+          st(c, v);
+          fft.template run_tab<+1>(w, j, sm, W, twt);
+          st(6 + c, w);
+          take(v);
+          fft.template run_tab<+1>(v, j, sm, W, twt);
+          st(3 + c, v);
+        }
+      } else {
+        take(v);  // A_w -> a_w and Ox = Y^-1(i ky A_w)
+#pragma unroll
+        for (int m = 0; m < V; ++m) w[m] = cmuli_s(v[m], kyv(m));
+        fft.template run_tab<+1>(v, j, sm, W, twt);
+        st(2, v);
+        fft.template run_tab<+1>(w, j, sm, W, twt);
+        st(5, w);
+        take(v);  // A_u -> a_u and Oz = Y^-1(Q_z - i ky A_u)
+        take(w);
+#pragma unroll
+        for (int m = 0; m < V; ++m) w[m] = csub(w[m], cmuli_s(v[m], kyv(m)));
+        fft.template run_tab<+1>(v, j, sm, W, twt);
+        st(0, v);
+        fft.template run_tab<+1>(w, j, sm, W, twt);
+        st(4, w);
+        take(v);
+        fft.template run_tab<+1>(v, j, sm, W, twt);
+        st(1, v);
+        take(v);
+        fft.template run_tab<+1>(v, j, sm, W, twt);
+        st(3, v);
+      }
+      continue;
+    }
     if (!LES) {
       C v[V];
 #pragma unroll 1
       for (int c = 0; c < 3; ++c) {
-        ld(c, v);
-        fft.template run<-1>(v, j, sm, W);
+        take(v);
+        fft.template run_tab<-1>(v, j, sm, W, twt);
         st(c, v);
       }
       continue;
     }
     const Tp kz2 = (Tp)(2 * col);
-    auto ky2 = [&](int m) { return (Tp)(2 * kc2c(j + T * m, N)); };
-    C t[V], acc[V], acc2[V];
+    C tt[V], acc[V], acc2[V];
     // G_x = N_x + 2i(ky F_xy + kz F_xz);  H_y = F_xy, H_z = F_xz, H_x = F_xx
-    ld(4, t);
-    fft.template run<-1>(t, j, sm, W);
-    st(4, t);
+    take(tt);
+    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    st(4, tt);
 #pragma unroll
-    for (int m = 0; m < V; ++m) acc[m] = cmuli_s(t[m], ky2(m));
-    ld(5, t);
-    fft.template run<-1>(t, j, sm, W);
-    st(5, t);
+    for (int m = 0; m < V; ++m) acc[m] = cmuli_s(tt[m], (Tp)2 * kyv(m));
+    take(tt);
+    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    st(5, tt);
 #pragma unroll
-    for (int m = 0; m < V; ++m) acc[m] = cadd(acc[m], cmuli_s(t[m], kz2));
-    ld(0, t);
-    fft.template run<-1>(t, j, sm, W);
+    for (int m = 0; m < V; ++m) acc[m] = cadd(acc[m], cmuli_s(tt[m], kz2));
+    take(tt);
+    fft.template run_tab<-1>(tt, j, sm, W, twt);
 #pragma unroll
-    for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc[m]);
-    st(0, t);
-    ld(3, t);
-    fft.template run<-1>(t, j, sm, W);
-    st(3, t);
+    for (int m = 0; m < V; ++m) tt[m] = cadd(tt[m], acc[m]);
+    st(0, tt);
+    take(tt);
+    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    st(3, tt);
     // G_y = N_y + 2i(ky F_yy + kz F_yz);  G_z = N_z + 2i(ky F_yz + kz F_zz)
-    ld(6, t);
-    fft.template run<-1>(t, j, sm, W);
+    take(tt);
+    fft.template run_tab<-1>(tt, j, sm, W, twt);
 #pragma unroll
-    for (int m = 0; m < V; ++m) acc[m] = cmuli_s(t[m], ky2(m));
-    ld(7, t);
-    fft.template run<-1>(t, j, sm, W);
+    for (int m = 0; m < V; ++m) acc[m] = cmuli_s(tt[m], (Tp)2 * kyv(m));
+    take(tt);
+    fft.template run_tab<-1>(tt, j, sm, W, twt);
 #pragma unroll
     for (int m = 0; m < V; ++m) {
-      acc[m] = cadd(acc[m], cmuli_s(t[m], kz2));
-      acc2[m] = cmuli_s(t[m], ky2(m));
+      acc[m] = cadd(acc[m], cmuli_s(tt[m], kz2));
+      acc2[m] = cmuli_s(tt[m], (Tp)2 * kyv(m));
     }
-    ld(1, t);
-    fft.template run<-1>(t, j, sm, W);
+    take(tt);
+    fft.template run_tab<-1>(tt, j, sm, W, twt);
 #pragma unroll
-    for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc[m]);
-    st(1, t);
-    ld(8, t);
-    fft.template run<-1>(t, j, sm, W);
+    for (int m = 0; m < V; ++m) tt[m] = cadd(tt[m], acc[m]);
+    st(1, tt);
+    take(tt);
+    fft.template run_tab<-1>(tt, j, sm, W, twt);
 #pragma unroll
-    for (int m = 0; m < V; ++m) acc2[m] = cadd(acc2[m], cmuli_s(t[m], kz2));
-    ld(2, t);
-    fft.template run<-1>(t, j, sm, W);
+    for (int m = 0; m < V; ++m) acc2[m] = cadd(acc2[m], cmuli_s(tt[m], kz2));
+    take(tt);
+    fft.template run_tab<-1>(tt, j, sm, W, twt);
 #pragma unroll
-    for (int m = 0; m < V; ++m) t[m] = cadd(t[m], acc2[m]);
-    st(2, t);
+    for (int m = 0; m < V; ++m) tt[m] = cadd(tt[m], acc2[m]);
+    st(2, tt);
   }
 }
 

@@ -12,7 +12,8 @@ import os
 import torch
 
 LIB_NAME = "libsles_b200.so"
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+# SLES_LIB_PATH selects another build of the library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("SLES_LIB_PATH") or os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
 SLES_F32, SLES_F64 = 0, 1
 LES_NONE, LES_SMAGORINSKY, LES_VREMAN = 0, 1, 2
