@@ -38,7 +38,7 @@ k_c2c_axis(const typename CT<Tp>::C* src, typename CT<Tp>::C* dst,  // may alias
            int ncols, int nchunks, Tp scale) {
   using K = C2CAxis<Tp, N, W, G>;
   using C = typename K::C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   C* scr = reinterpret_cast<C*>(smem_raw);
   const int tid = threadIdx.x;
   const int l = tid % W, j = (tid / W) % K::T, g = tid / (W * K::T);
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(RealAxis<Tp, NR, LPB>::THREADS)
 k_r2c_line(const Tp* __restrict__ src, typename CT<Tp>::C* __restrict__ dst, long long nlines, int NKP) {
   using K = RealAxis<Tp, NR, LPB>;
   using C = typename K::C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   C* twN = reinterpret_cast<C*>(smem_raw);
   C* scr = twN + K::L;
   fill_twN<Tp, NR>(twN);
@@ -118,7 +118,7 @@ k_c2r_line(const typename CT<Tp>::C* __restrict__ src, Tp* __restrict__ dst, lon
            Tp scale) {
   using K = RealAxis<Tp, NR, LPB>;
   using C = typename K::C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   C* twN = reinterpret_cast<C*>(smem_raw);
   C* scr = twN + K::L;
   fill_twN<Tp, NR>(twN);

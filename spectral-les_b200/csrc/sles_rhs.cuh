@@ -237,7 +237,7 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
   using K = XGeo<Tp, N, F, DIM>;
   using C = typename CT<Tp>::C;
   constexpr int T = K::T, V = K::V, D = DIM, W = K::W;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   C* rst = reinterpret_cast<C*>(smem_raw);  // [D][N][W] projected components
   C* sm0 = rst + D * K::TE;                 // exchange scratch
   C* twt = sm0 + K::SCR;                    // twiddle table exp(-2 pi i e/N)
@@ -691,7 +691,7 @@ k_zpass(const ZArgs<Tp> A) {
   using F = typename K::F;
   using C = typename CT<Tp>::C;
   constexpr int T = K::T, V = K::V, NKP = K::NKP, SFS = LPI * K::RS;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
   C* twN = reinterpret_cast<C*>(smem_raw + K::OFF_TW);
   C* stage = reinterpret_cast<C*>(smem_raw + K::OFF_STAGE);   // [2][NIN][LPI][NKP]
