@@ -167,6 +167,30 @@ int sles_diag(sles_plan* plan, const void* u_hat, const void* u_phys, double* ou
 int sles_profile_rhs(sles_plan* plan, const void* u_hat, void* du_scratch, int iters, double* ms,
                      void* stream);
 
+/*
+ * The fused RHS evaluation of sles_rhs for callers that cannot allocate device
+ * memory: code that runs where cudaMalloc is off limits (inside an allocator
+ * callback, a host application that owns every device allocation through its
+ * own pool, a latency-critical loop that must not hit cudaMalloc's implicit
+ * synchronization).  No counterpart in the reference.  The scratch is a
+ * file-scope device array of SLES_STATIC_WORKSPACE_BYTES inside the library
+ * instead of the plan's workspace, so the plan needs no sles_plan_set_workspace
+ * for this call; inputs and outputs are still the caller's.  Plans whose
+ * workspace (sles_plan_workspace_bytes) exceeds the array are rejected with
+ * SLES_ERR_WORKSPACE before anything runs (e.g. 3D LES up to N = 64 in float64,
+ * N = 64 in float32; 3D without LES and 2D go further).
+ * The first call on a device looks up the array's device address with that
+ * device current; make that first call before any stream capture.  Every GPU
+ * that loads the library holds the array until the process exits.  All calls on
+ * a device share the array and it keeps the last call's contents (each call
+ * clears the part that must start at zero); calls whose work overlaps on the
+ * GPU race on it and must be serialized by the caller.  No cudaMalloc, cudaFree
+ * or allocating library call is made.
+ */
+#define SLES_STATIC_WORKSPACE_BYTES (32u << 20)
+int sles_rhs_static_workspace(sles_plan* plan, const void* u_hat, const void* u_phys, const void* curl_phys,
+                              void* du_out, void* f1_out, void* stream);
+
 /* Human-readable text for a status code (static storage). */
 const char* sles_status_string(int status);
 int sles_version(void);

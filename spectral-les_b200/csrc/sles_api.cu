@@ -186,3 +186,51 @@ int sles_profile_rhs(sles_plan* p, const void* uh, void* du, int iters, double* 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// sles_rhs_static_workspace: the fused RHS evaluation for callers that cannot
+// allocate device memory (no counterpart in the reference).  Its scratch is
+// this file-scope device array instead of a caller-provided workspace, so the
+// call makes no cudaMalloc/cudaFree and no allocating library call.  Every GPU
+// that loads this library holds the array (SLES_STATIC_WORKSPACE_BYTES) until
+// the process exits.  All calls on a device share it and it keeps the previous
+// call's contents; the only part that must start at zero (the error word) is
+// cleared by each call.  Calls whose work overlaps on the GPU (two streams, two
+// threads) race on the array and must be serialized by the caller.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_sles_static_ws[SLES_STATIC_WORKSPACE_BYTES];
+
+namespace {
+std::mutex g_static_ws_mu;
+constexpr int kMaxDevices = 64;
+void* g_static_ws_addr[kMaxDevices] = {};  // device address of g_sles_static_ws, per device ordinal
+}  // namespace
+
+extern "C" int sles_rhs_static_workspace(sles_plan* p, const void* uh, const void* uphys, const void* cphys,
+                                         void* du, void* f1, void* stream) {
+  if (!p || !uh || !du) return SLES_ERR_INVALID_ARG;
+  if (sles_plan_workspace_bytes(p) > (size_t)SLES_STATIC_WORKSPACE_BYTES) return SLES_ERR_WORKSPACE;
+  if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return SLES_ERR_CUDA;
+  if (dev < 0 || dev >= kMaxDevices) return SLES_ERR_UNSUPPORTED;
+  void* ws = nullptr;
+  {
+    // first call on a device: look up the array's device address with that
+    // device current (in host code the array's name is only a host-side stand-in)
+    std::lock_guard<std::mutex> g(g_static_ws_mu);
+    if (!g_static_ws_addr[dev]) {
+      void* a = nullptr;
+      if (cudaGetSymbolAddress(&a, g_sles_static_ws) != cudaSuccess || !a) return SLES_ERR_CUDA;
+      g_static_ws_addr[dev] = a;
+    }
+    ws = g_static_ws_addr[dev];
+  }
+  sles::PlanInfo info = p->info;  // the plan's own workspace (if any) is left untouched
+  info.ws = ws;
+  info.ws_bytes = SLES_STATIC_WORKSPACE_BYTES;
+  info.flags = reinterpret_cast<unsigned*>(ws);
+  info.scal = reinterpret_cast<double*>(reinterpret_cast<char*>(ws) + 256);
+  if (cudaMemsetAsync(info.flags, 0, sizeof(unsigned), (cudaStream_t)stream) != cudaSuccess) return SLES_ERR_CUDA;
+  return p->eng->rhs(info, uh, uphys, cphys, du, f1, (cudaStream_t)stream);
+}

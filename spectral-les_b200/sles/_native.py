@@ -24,7 +24,7 @@ EXPORTED = [
     "sles_plan_create", "sles_plan_destroy", "sles_plan_layout", "sles_plan_workspace_bytes",
     "sles_plan_set_workspace", "sles_plan_set_params", "sles_fft_r2c", "sles_fft_c2r",
     "sles_velocity_curl", "sles_velocity_gradient", "sles_rhs", "sles_stage", "sles_diag",
-    "sles_status_string", "sles_version", "sles_profile_rhs",
+    "sles_status_string", "sles_version", "sles_profile_rhs", "sles_rhs_static_workspace",
 ]
 
 
@@ -75,6 +75,7 @@ def load_library(path: str = LIB_PATH):
         "sles_diag": (i, [vp, vp, vp, vp, vp, i, vp]),
         "sles_status_string": (ctypes.c_char_p, [i]),
         "sles_profile_rhs": (i, [vp, vp, vp, i, vp, vp]),
+        "sles_rhs_static_workspace": (i, [vp, vp, vp, vp, vp, vp, vp]),
         "sles_version": (i, []),
     }
     for name, (res, args) in sig.items():
