@@ -225,7 +225,11 @@ template <typename Tp, int N, int DIM>
 struct EngineImpl final : Engine {
   using C = typename CT<Tp>::C;
   using TR = Transforms<Tp, N, DIM>;
-  using FX = typename PlanLo<Tp, N>::F;
+#ifndef SLES_X_PADD
+#define SLES_X_PADD 16
+#endif
+  // x pass: exchange padding divisor SLES_X_PADD (0: the plan's first radix)
+  using FX = typename WithPad<typename PlanLo<Tp, N>::F, SLES_X_PADD>::F;
   using FY = typename PlanLo<Tp, N>::F;
   static constexpr int W = XGeo<Tp, N, FX, DIM>::W;
   static constexpr int TZ = PlanFor<Tp, N / 2>::F::T;

@@ -145,14 +145,13 @@ __device__ __forceinline__ void dft(C (&u)[R]) {
   }
 }
 
-// padded position in an exchange line: one pad slot after every 16 points
-__device__ __forceinline__ int xpad(int p) { return p + (p >> 4); }
-__host__ __device__ constexpr int xline_len(int L) { return L + L / 16 + 1; }
 
 // ---------------------------------------------------------------------------
 // Stockham line engine
 // ---------------------------------------------------------------------------
-template <typename Tp, int L_, int R0, int R1, int R2, int T_>
+// PADD: one exchange pad slot after every PADD points (0: PADD = R0, which
+// keeps the first stage's autosort writes, stride R0, on distinct banks)
+template <typename Tp, int L_, int R0, int R1, int R2, int T_, int PADD_ = 0>
 struct LineFFT {
   using C = typename CT<Tp>::C;
   static constexpr int L = L_;
@@ -166,6 +165,13 @@ struct LineFFT {
   static constexpr int NB2 = (S >= 3) ? (L / R2) / T : 0;
   static constexpr int TW1 = (S >= 2) ? NB1 * (R1 - 1) : 1;
   static constexpr int TW2 = (S >= 3) ? NB2 * (R2 - 1) : 1;
+  static constexpr int PADD = PADD_ > 0 ? PADD_ : R0;
+  static constexpr int XLEN = L + L / PADD + 1;  // exchange line length (slots)
+  __device__ __forceinline__ static int pad(int p) { return p + (int)((unsigned)p / (unsigned)PADD); }
+  // per-stage twiddle tables, [r][k] so a warp reads consecutive entries:
+  // stage 1: W_{R0 R1}^{k r}, k < R0; stage 2: W_L^{k r}, k < R0 R1
+  static constexpr int TAB1 = (S >= 2) ? (R1 - 1) * R0 : 0;
+  static constexpr int TAB = TAB1 + ((S >= 3) ? (R2 - 1) * R0 * R1 : 0) + 1;
 
   C tw1[TW1];
   C tw2[TW2];
@@ -210,32 +216,31 @@ struct LineFFT {
 #pragma unroll
         for (int r = 0; r < R; ++r) v[q + r * NB] = u[r];
       } else {
-        int b = j + T * q;
-        int k = b % Ns;
-        int idxD = (b / Ns) * Ns * R + k;
+        const unsigned b = (unsigned)(j + T * q), ns = (unsigned)Ns;
+        const int idxD = (int)((b / ns) * ns * R + b % ns);
 #pragma unroll
-        for (int r = 0; r < R; ++r) sm[xpad(idxD + r * Ns) * ws] = u[r];
+        for (int r = 0; r < R; ++r) sm[pad(idxD + r * Ns) * ws] = u[r];
       }
     }
   }
 
   // Same stage with twiddles read from a shared table tab[e] = exp(-2 pi i e/L)
   // (threads of one line share j, so a warp reads few distinct entries).
-  template <int R, int DIR, bool LAST>
+  // LIN: tab is the linear table W_L^e (e < L) instead of the per-stage [r][k] tables
+  template <int R, int DIR, bool LAST, bool LIN>
   __device__ __forceinline__ void stage_tab(C (&v)[V], const C* tab, int Ns, int j, C* sm, int ws) {
     constexpr int NB = (L / R) / T;
-    const int stride = L / (Ns * R);
 #pragma unroll
     for (int q = 0; q < NB; ++q) {
       C u[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) u[r] = v[q + r * NB];
-      const int b = j + T * q;
-      const int k = b % Ns;
-      if (Ns > 1) {
+      const unsigned b = (unsigned)(j + T * q), ns = (unsigned)Ns;
+      const int k = (int)(b % ns);
+      if (Ns > 1) {  // tab points at this stage's [r-1][k] table (Ns entries per r)
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          const C w = tab[k * r * stride];
+          const C w = LIN ? tab[k * r * (L / (Ns * R))] : tab[(r - 1) * Ns + k];
           u[r] = (DIR < 0) ? cmul(u[r], w) : cmulc(u[r], w);
         }
       }
@@ -244,42 +249,55 @@ struct LineFFT {
 #pragma unroll
         for (int r = 0; r < R; ++r) v[q + r * NB] = u[r];
       } else {
-        const int idxD = (b / Ns) * Ns * R + k;
+        const int idxD = (int)((b / ns) * ns * R) + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) sm[xpad(idxD + r * Ns) * ws] = u[r];
+        for (int r = 0; r < R; ++r) sm[pad(idxD + r * Ns) * ws] = u[r];
       }
     }
   }
 
   // Transform with twiddles from `tab` (L entries, see fill_table); needs no init().
-  template <int DIR>
+  template <int DIR, bool LIN = false>
   __device__ __forceinline__ void run_tab(C (&v)[V], int j, C* sm, int ws, const C* tab) {
     if constexpr (S >= 2) __syncthreads();
-    stage_tab<R0, DIR, S == 1>(v, tab, 1, j, sm, ws);
+    stage_tab<R0, DIR, S == 1, LIN>(v, tab, 1, j, sm, ws);
     if constexpr (S >= 2) {
       exchange(v, j, sm, ws);
       if constexpr (S >= 3) __syncthreads();
-      stage_tab<R1, DIR, S == 2>(v, tab, R0, j, sm, ws);
+      stage_tab<R1, DIR, S == 2, LIN>(v, tab, R0, j, sm, ws);
     }
     if constexpr (S >= 3) {
       exchange(v, j, sm, ws);
-      stage_tab<R2, DIR, true>(v, tab, R0 * R1, j, sm, ws);
+      stage_tab<R2, DIR, true, LIN>(v, LIN ? tab : tab + TAB1, R0 * R1, j, sm, ws);
     }
   }
 
-  // cooperative fill of the twiddle table (float64, rounded once)
-  __device__ __forceinline__ static void fill_table(C* tab) {
+  // linear table W_L^e, e < L (float64, rounded once)
+  __device__ __forceinline__ static void fill_table_lin(C* tab) {
     for (int e = threadIdx.x; e < L; e += blockDim.x) tab[e] = twiddle<Tp>(e, L, -1);
+  }
+
+  // cooperative fill of the per-stage twiddle tables (TAB entries; float64, rounded once)
+  __device__ __forceinline__ static void fill_table(C* tab) {
+    for (int e = threadIdx.x; e < TAB; e += blockDim.x) {
+      if (e < TAB1) {
+        const int r = e / R0 + 1, k = e % R0;
+        tab[e] = twiddle<Tp>((long long)k * r, R0 * R1, -1);
+      } else if (e < TAB - 1) {
+        const int f = e - TAB1, r = f / (R0 * R1) + 1, k = f % (R0 * R1);
+        tab[e] = twiddle<Tp>((long long)k * r, L, -1);
+      }
+    }
   }
 
   __device__ __forceinline__ void exchange(C (&v)[V], int j, C* sm, int ws) {
     __syncthreads();
 #pragma unroll
-    for (int m = 0; m < V; ++m) v[m] = sm[xpad(j + T * m) * ws];
+    for (int m = 0; m < V; ++m) v[m] = sm[pad(j + T * m) * ws];
   }
 
   // In-place transform of the cyclic registers.  sm: this line's exchange
-  // scratch (xline_len(L) slots of stride ws).  All threads of the block must
+  // scratch (XLEN slots of stride ws).  All threads of the block must
   // call this uniformly (it contains __syncthreads when S > 1).  Convention
   // shared by every user of an exchange scratch: a barrier precedes each
   // write phase, so back-to-back transforms on one scratch are safe.
@@ -317,6 +335,13 @@ template <typename Tp> struct PlanFor<Tp, 128>  { using F = LineFFT<Tp, 128, 16,
 template <typename Tp> struct PlanFor<Tp, 256>  { using F = LineFFT<Tp, 256, 16, 16, 1, 16>; };
 template <typename Tp> struct PlanFor<Tp, 512>  { using F = LineFFT<Tp, 512, 16, 16, 2, 32>; };
 template <typename Tp> struct PlanFor<Tp, 1024> { using F = LineFFT<Tp, 1024, 16, 16, 4, 64>; };
+
+// the same plan with another exchange padding divisor
+template <class F, int P> struct WithPad;
+template <typename Tp, int L, int R0, int R1, int R2, int T, int P0, int P>
+struct WithPad<LineFFT<Tp, L, R0, R1, R2, T, P0>, P> {
+  using F = LineFFT<Tp, L, R0, R1, R2, T, P>;
+};
 
 // Plans with at most 8-12 points per thread, for passes that keep several
 // transformed lines live in registers at once (one more exchange per line).
@@ -357,13 +382,13 @@ __device__ __forceinline__ void r2c_post(typename F::C (&v)[F::V], int j, typena
   using Tp = decltype(C::x);
   __syncthreads();
 #pragma unroll
-  for (int m = 0; m < F::V; ++m) sm[xpad(j + F::T * m) * ws] = v[m];
+  for (int m = 0; m < F::V; ++m) sm[F::pad(j + F::T * m) * ws] = v[m];
   __syncthreads();
 #pragma unroll
   for (int m = 0; m < F::V; ++m) {
     int k = j + F::T * m;
     C z = v[m];
-    C zc = cconj(sm[xpad((F::L - k) % F::L) * ws]);
+    C zc = cconj(sm[F::pad((int)((unsigned)(F::L - k) % (unsigned)F::L)) * ws]);
     C s = cadd(z, zc), d = csub(z, zc);
     C t = cmulmi(cmul(twN[k], d));
     out(k, cmk<C>((Tp)0.5 * (s.x + t.x), (Tp)0.5 * (s.y + t.y)));

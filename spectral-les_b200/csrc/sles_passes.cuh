@@ -27,7 +27,7 @@ struct C2CAxis {
   static constexpr int T = F::T;
   static constexpr int V = F::V;
   static constexpr int THREADS = G * W * T;
-  static constexpr int SCR = xline_len(N) * W;  // per item
+  static constexpr int SCR = F::XLEN * W;  // per item
   static constexpr size_t SMEM = (size_t)G * SCR * sizeof(C);
 };
 
@@ -79,7 +79,7 @@ struct RealAxis {
   static constexpr int L = NR / 2;
   static constexpr int T = F::T;
   static constexpr int THREADS = LPB * T;
-  static constexpr int LS = ((xline_len(L) + 15) / 16) * 16 + 8;  // line stride of the scratch
+  static constexpr int LS = ((F::XLEN + 15) / 16) * 16 + 8;  // line stride of the scratch
   static constexpr size_t SMEM = ((size_t)LPB * LS + L) * sizeof(C);
 };
 

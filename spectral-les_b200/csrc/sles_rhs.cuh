@@ -188,10 +188,10 @@ struct TGeo {
   static constexpr int NBUF =
       NBUF_SET > 0 ? NBUF_SET : ((TE * sizeof(C) <= 16384) ? 4 : ((TE * sizeof(C) <= 32768) ? 3 : 2));
   static constexpr unsigned BOX_BYTES = RB * W * sizeof(C);
-  static constexpr int SCR = xline_len(N) * W;
+  static constexpr int SCR = F::XLEN * W;
   using Ring = TileRing<C, NBUF, TE>;
   static constexpr size_t RING_BYTES = RING ? Ring::bytes() : 0;
-  static constexpr size_t SMEM = RING_BYTES + ((size_t)SCR + N) * sizeof(C);  // + twiddle table
+  static constexpr size_t SMEM = RING_BYTES + ((size_t)SCR + F::TAB) * sizeof(C);  // + twiddle tables
 #ifndef SLES_T_MINB256
 #define SLES_T_MINB256 2
 #endif
@@ -207,8 +207,8 @@ struct XGeo {
   static constexpr int T = F::T, V = F::V;
   static constexpr int THREADS = W * T;
   static constexpr int TE = N * W;
-  static constexpr int SCR = xline_len(N) * W;
-  static constexpr size_t SMEM = ((size_t)DIM * TE + SCR + N) * sizeof(C);
+  static constexpr int SCR = F::XLEN * W;
+  static constexpr size_t SMEM = ((size_t)DIM * TE + SCR + N) * sizeof(C);  // + linear twiddle table
 #ifndef SLES_X_MINB256
 #define SLES_X_MINB256 2
 #endif
@@ -243,7 +243,7 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
   C* twt = sm0 + K::SCR;                    // twiddle table exp(-2 pi i e/N)
   const int tid = threadIdx.x;
   const int l = tid % W, j = tid / W;
-  F::fill_table(twt);
+  F::fill_table_lin(twt);
   __syncthreads();
   F fft;
   const int nsl = (DIM == 3) ? N : 1;
@@ -276,17 +276,17 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
         C b[V];
 #pragma unroll
         for (int m = 0; m < V; ++m) b[m] = cmuli_s(s[m], (Tp)kx_at(m));  // i kx u_c
-        fft.template run_tab<+1>(b, j, sm, W, twt);
+        fft.template run_tab<+1, true>(b, j, sm, W, twt);
         st(D + c, b);
       } else if ((DIM == 3 && c >= 1) || (DIM == 2 && c == 1)) {
         C q[V];
         const Tp sg = (DIM == 3 && c == 2) ? (Tp)-1 : (Tp)1;  // 3D: -i kx w -> [3], i kx v -> [4]; 2D: i kx v -> [2]
 #pragma unroll
         for (int m = 0; m < V; ++m) q[m] = cmuli_s(s[m], sg * (Tp)kx_at(m));
-        fft.template run_tab<+1>(q, j, sm, W, twt);
+        fft.template run_tab<+1, true>(q, j, sm, W, twt);
         st(DIM == 3 ? (c == 2 ? 3 : 4) : 2, q);
       }
-      fft.template run_tab<+1>(s, j, sm, W, twt);
+      fft.template run_tab<+1, true>(s, j, sm, W, twt);
       st(c, s);
     };
     if (!A.fwd) {
@@ -303,11 +303,11 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
     for (int c = 0; c < D; ++c) {
       C v[V];
       ld(v, ws, c);
-      fft.template run_tab<-1>(v, j, sm, W, twt);
+      fft.template run_tab<-1, true>(v, j, sm, W, twt);
       if (LES && DIM == 3) {  // + 2i kx F_cx
         C h[V];
         ld(h, ws, 3 + c);
-        fft.template run_tab<-1>(h, j, sm, W, twt);
+        fft.template run_tab<-1, true>(h, j, sm, W, twt);
 #pragma unroll
         for (int m = 0; m < V; ++m) v[m] = cadd(v[m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
       }
@@ -320,11 +320,11 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
       const Tp ky2 = (Tp)(2 * col);
       C h[V];
       ld(h, ws, 2);
-      fft.template run_tab<-1>(h, j, sm, W, twt);
+      fft.template run_tab<-1, true>(h, j, sm, W, twt);
 #pragma unroll
       for (int m = 0; m < V; ++m) rst[rpos(0, m)] = cadd(rst[rpos(0, m)], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
       ld(h, ws, 3);
-      fft.template run_tab<-1>(h, j, sm, W, twt);
+      fft.template run_tab<-1, true>(h, j, sm, W, twt);
 #pragma unroll
       for (int m = 0; m < V; ++m) {
         rst[rpos(0, m)] = cadd(rst[rpos(0, m)], cmuli_s(h[m], ky2));
@@ -332,7 +332,7 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
       }
       if (!PAR2D) {
         ld(h, ws, 4);
-        fft.template run_tab<-1>(h, j, sm, W, twt);
+        fft.template run_tab<-1, true>(h, j, sm, W, twt);
 #pragma unroll
         for (int m = 0; m < V; ++m) rst[rpos(1, m)] = cadd(rst[rpos(1, m)], cmuli_s(h[m], ky2));
       }
@@ -583,7 +583,7 @@ struct ZGeo {
   // per (field, line) region: the line's FFT exchange scratch (LS complex,
   // LS = 8 mod 16 keeps the autosort writes conflict-free) and, between the
   // transforms, the physical line itself (N reals)
-  static constexpr int LS = ((xline_len(L) + 15) / 16) * 16 + 8;
+  static constexpr int LS = ((F::XLEN + 15) / 16) * 16 + 8;
   static constexpr int RS = 2 * LS;
   static_assert(RS >= N, "region must hold a physical line");
   static constexpr int STAGE = NIN * LPI * NKP;   // complex elements per staging buffer
