@@ -132,18 +132,106 @@ def gpu_index():
 # ---------------------------------------------------------------------------
 # the fused path
 # ---------------------------------------------------------------------------
-def make_domain(n, dtype, seed):
+def make_domain(n, dtype, seed, method="RK3", les="Smagorinsky", nu=NU, cs=CS, dt=DT, k0=K0, parity=True):
     import torch
     from sles.initialize_domain import InitializeDomain
     from sles.initial import initial_velocity
     from sles.synthetic import random_spectrum_velocity
-    d = InitializeDomain(nu=NU, dimension=3, time_stepSize=DT, No_of_gridpoint=4 * n, method="RK3", LES_ON=1,
-                         LES_model="Smagorinsky", Cs=CS, dtype=dtype)
-    u, v, w = random_spectrum_velocity(n, K0, U0, seed=seed)
+    d = InitializeDomain(nu=nu, dimension=3, time_stepSize=dt, No_of_gridpoint=(4 if les else 1) * n, method=method,
+                         LES_ON=1 if les else 0, LES_model=les, Cs=cs, dtype=dtype, parity_mode=parity)
+    u, v, w = random_spectrum_velocity(n, k0, U0, seed=seed)
     initial_velocity(d, u, v, w)
     del u, v, w
     torch.cuda.synchronize()
     return d
+
+
+def spectrum_error(a, b, n):
+    """max_k |E_a(k) - E_b(k)| / E_b(k) over integer shells 1..floor(2/3 (N/2+1))."""
+    from sles.adjoint import shell_spectrum
+    kc = int(2.0 / 3.0 * (n // 2 + 1))
+    ea, eb = shell_spectrum(a, n, kc + 1)[1:], shell_spectrum(b, n, kc + 1)[1:]
+    return float(((ea - eb).abs() / eb).max())
+
+
+def rel_l2(a, b):
+    import torch
+    return float(torch.linalg.vector_norm(a.to(b.dtype) - b) / torch.linalg.vector_norm(b))
+
+
+def bench_512(peak, rank):
+    """512^3 cases: the Smagorinsky LES recipe (RK3, cfg-2 parameters) at 512^3
+    against the plain FP64 GPU path and FP64 fused after 100 steps; and the
+    Vreman ETD2 case (k0=6, nu=5e-5, c=0.07 i.e. Cs=sqrt(0.028), dt=5e-4,
+    corrected ETD2 with float64 phi-coefficients), FP32 against FP64 after 100
+    steps, with per-kernel times."""
+    import torch
+    from sles import ETD2_method, RK3_method
+    n, npts, out = 512, 512.0 ** 3, {}
+    step = RK3_method.solveForNextTimestep
+    # -- Smagorinsky RK3 at 512^3
+    d32 = make_domain(n, "float32", rank)
+    d64 = make_domain(n, "float64", rank)
+    for _ in range(3):
+        step(d32)
+        step(d64)
+    t32 = time_steps(d32, 20, step)
+    t64 = time_steps(d64, 20, step)
+    for _ in range(100 - 23):
+        step(d32)
+        step(d64)
+    err = rel_l2(d32.U_hat, d64.U_hat)
+    ek = spectrum_error(d32.U_hat, d64.U_hat, n)
+    kms = d32._plan.profile_rhs(d32._s_uhat, d32._new_hc(3), 10)
+    del d32, d64
+    torch.cuda.empty_cache()
+    tp = torch_plain_fp64_rk3(n, 2, 1, rank)
+    torch.cuda.empty_cache()
+    v32, v64, vtp = npts * 20 / t32 / 1e6, npts * 20 / t64 / 1e6, npts / tp / 1e6
+    ms = t32 / 20 * 1e3
+    out["smagorinsky_rk3"] = {
+        "value": round(v32, 2), "unit": UNIT, "ms_per_step": round(ms, 3),
+        "fused_fp64_value": round(v64, 2), "torch_fft_fp64_value": round(vtp, 2),
+        "speedup_vs_torch_fp64": round(v32 / vtp, 2), "speedup_vs_fused_fp64": round(v32 / v64, 2),
+        "rel_l2_fp32_vs_fp64_after_100_steps": err, "ek_err_fp32_vs_fp64_after_100_steps": ek,
+        "step_roofline_frac": round(STEP_BYTES_PER_PT_RHS["f32"] * 3 * npts / (ms * 1e-3) / 1e9 / peak, 4),
+        "kernel_ms": dict(zip(["x_inverse", "y_inverse", "z_fused", "y_forward", "x_forward_combine"],
+                              [round(x, 4) for x in kms])),
+        "config": "512^3, random-phase spectrum k0=4, nu=1e-4, Smagorinsky Cs=0.17, reference RK3, dt=1e-3"}
+    # -- Vreman ETD2 at 512^3
+    cs_v = math.sqrt(0.07 / 2.5)
+    mk = lambda dt_: make_domain(n, dt_, rank, method="ETD2", les="vreman", nu=5e-5, cs=cs_v, dt=5e-4, k0=6.0,
+                                 parity=False)
+    estep = ETD2_method.solveForNextTimestep
+    d32, d64 = mk("float32"), mk("float64")
+    for _ in range(3):
+        estep(d32)
+        estep(d64)
+    t32 = time_steps(d32, 20, estep)
+    t64 = time_steps(d64, 20, estep)
+    for _ in range(100 - 23):
+        estep(d32)
+        estep(d64)
+    err = rel_l2(d32.U_hat, d64.U_hat)
+    ek = spectrum_error(d32.U_hat, d64.U_hat, n)
+    kms = d32._plan.profile_rhs(d32._s_uhat, d32._new_hc(3), 10)
+    fbytes = float(n) * n * (n // 2 + 1) * 8
+    algb = {"x_inverse": 9 * fbytes, "y_inverse": 15 * fbytes, "z_fused": 18 * fbytes, "y_forward": 15 * fbytes,
+            "x_forward_combine": 18 * fbytes}
+    names = ["x_inverse", "y_inverse", "z_fused", "y_forward", "x_forward_combine"]
+    del d32, d64
+    torch.cuda.empty_cache()
+    ms = t32 / 20 * 1e3
+    out["vreman_etd2"] = {
+        "value": round(npts * 20 / t32 / 1e6, 2), "unit": UNIT, "ms_per_step": round(ms, 3),
+        "fused_fp64_value": round(npts * 20 / t64 / 1e6, 2),
+        "rel_l2_fp32_vs_fp64_after_100_steps": err, "ek_err_fp32_vs_fp64_after_100_steps": ek,
+        "step_roofline_frac": round(STEP_BYTES_PER_PT_RHS["f32"] * 1 * npts / (ms * 1e-3) / 1e9 / peak, 4),
+        "kernel_ms": dict(zip(names, [round(x, 4) for x in kms])),
+        "kernel_gbs": {k: round(algb[k] / (t * 1e-3) / 1e9, 1) for k, t in zip(names, kms)},
+        "config": "512^3, random-phase spectrum k0=6, nu=5e-5, Vreman c=0.07 (Cs=%.5f), ETD2 (Cox-Matthews, "
+                  "float64 phi coefficients), dt=5e-4" % cs_v}
+    return out
 
 
 def time_steps(d, k, step):
@@ -251,6 +339,129 @@ def run_reference(args, rank, world):
                             "sample": sample},
            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
+
+
+def bench_adjoint(rank):
+    """Adjoint case: 128^3 Smagorinsky LES, RK4, nu=2e-4, dt=2e-3, 100 steps,
+    FP32 forward and FP32 adjoint with checkpoints every 10 steps.  Loss
+    sum_k (log E(k,T) - log E_target(k))^2 over shells 1..43; E_target from a
+    256^3 FP64 no-LES RK4 run of the same recipe and seed to T=0.2 (shells
+    1..43 lie inside the 128^3 dealiased band).  Reports forward and backward
+    times (CUDA events) and the gradients' agreement with the FP64 adjoint and
+    with a central difference in Cs (eps=1e-3, FP64)."""
+    import torch
+    from sles import RK4_method
+    from sles.adjoint import RK4Rollout, log_spectrum_misfit, shell_spectrum
+    n, nu, dt, steps, cs = 128, 2e-4, 2e-3, 100, CS
+    dT = make_domain(256, "float64", rank, method="RK4", les=None, nu=nu, dt=dt)
+    dT.U_hat1[...] = dT.U_hat
+    for _ in range(steps):
+        RK4_method.solveForNextTimestep(dT)
+    Et = shell_spectrum(dT.U_hat, 256, 44).detach()
+    del dT
+    d0 = make_domain(n, "float64", rank, method="RK4", nu=nu, dt=dt)
+    U0 = d0.U_hat.clone()
+    del d0
+    res = {}
+    for name, dtp in (("f32", torch.float32), ("f64", torch.float64)):
+        ro = RK4Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=dtp, checkpoint_every=10)
+        U = U0.to(ro.cdtype)
+        # gradient of the loss at U_T (torch autograd on the loss only), then timed sweeps
+        UT, _ = ro.forward_states(U, cs, steps)
+        UTv = UT[..., : ro.nk].clone().requires_grad_(True)
+        loss = log_spectrum_misfit(UTv, Et, n)
+        gUT, = torch.autograd.grad(loss, [UTv])
+        ro.timed(U, cs, steps, gUT)  # warm-up (allocations)
+        fw, bw = [], []
+        for _ in range(3):
+            f_ms, b_ms, _, g, c = ro.timed(U, cs, steps, gUT)
+            fw.append(f_ms)
+            bw.append(b_ms)
+        res[name] = dict(fwd_ms=min(fw), bwd_ms=min(bw), loss=float(loss), g=g[..., : ro.nk].to(torch.complex128),
+                         cs=float(c[0]), ro=ro, U=U)
+    r32, r64 = res["f32"], res["f64"]
+    # central difference in Cs on the FP64 path
+    ro, U = r64["ro"], r64["U"]
+    lo = lambda c: float(log_spectrum_misfit(ro.forward_states(U, c, steps)[0][..., : ro.nk], Et, n))
+    cd = lambda e: (lo(cs + e) - lo(cs - e)) / (2 * e)
+    fd1, fd2 = cd(1e-3), cd(5e-4)
+    fd = (4.0 * fd2 - fd1) / 3.0  # Richardson: O(eps^4) truncation
+    g32, g64 = r32["g"], r64["g"]
+    out = {"fwd_ms": round(r32["fwd_ms"], 2), "bwd_ms": round(r32["bwd_ms"], 2),
+           "adjoint_fwd_ratio": round(r32["bwd_ms"] / r32["fwd_ms"], 3),
+           "fwd_ms_f64": round(r64["fwd_ms"], 2), "bwd_ms_f64": round(r64["bwd_ms"], 2),
+           "adjoint_fwd_ratio_f64": round(r64["bwd_ms"] / r64["fwd_ms"], 3),
+           "loss": r32["loss"], "dL_dCs_f32": r32["cs"], "dL_dCs_f64": r64["cs"], "dL_dCs_central_diff_f64_eps1e-3": fd1,
+           "dL_dCs_richardson_f64": fd, "cs_rel_err_f64_vs_richardson": abs(r64["cs"] - fd) / abs(fd),
+           "cs_rel_err_f32_vs_richardson": abs(r32["cs"] - fd) / abs(fd),
+           "grad_u0_rel_l2_f32_vs_f64": rel_l2(g32, g64),
+           "config": "128^3, random-phase spectrum k0=4, nu=2e-4, Smagorinsky Cs=0.17, RK4, dt=2e-3, 100 steps, "
+                     "checkpoints every 10, loss on log E(k), k=1..43; backward = segment recompute + reverse stages"}
+    del res, r32, r64, ro, U
+    torch.cuda.empty_cache()
+    return out
+
+
+def ensemble_members(seed):
+    """48 members from one generator: 32 2D vorticity runs (N in {256, 512,
+    1024}, nu log-uniform in [1e-5, 1e-3], Gaussian vorticity peaked at k=10,
+    RK4, dt=1e-3) and 16 3D Smagorinsky runs (N in {64, 96, 128}, Cs uniform
+    in [0.1, 0.2], random-phase spectrum k0=4, nu=1e-4, RK4, dt=1e-3); FP32."""
+    import numpy as np
+    from sles.initial import initial_velocity, initial_vorticity
+    from sles.initialize_domain import InitializeDomain
+    from sles.synthetic import gaussian_vorticity_2d, random_spectrum_velocity
+    rng = np.random.default_rng(seed)
+    members = []
+    for i in range(32):
+        n = int(rng.choice([256, 512, 1024]))
+        nu = float(10.0 ** rng.uniform(-5, -3))
+        d = InitializeDomain(nu=nu, dimension=2, time_stepSize=1e-3, No_of_gridpoint=n, method="RK4",
+                             dtype="float32")
+        initial_vorticity(d, gaussian_vorticity_2d(n, seed=int(rng.integers(1 << 30)), kp=10.0))
+        members.append(d)
+    for i in range(16):
+        n = int(rng.choice([64, 96, 128]))
+        cs = float(rng.uniform(0.1, 0.2))
+        d = InitializeDomain(nu=NU, dimension=3, time_stepSize=1e-3, No_of_gridpoint=4 * n, method="RK4", LES_ON=1,
+                             LES_model="Smagorinsky", Cs=cs, dtype="float32")
+        initial_velocity(d, *random_spectrum_velocity(n, K0, U0, seed=int(rng.integers(1 << 30))))
+        members.append(d)
+    for d in members:
+        d.U_hat1[...] = d.U_hat
+    return members
+
+
+def bench_ensemble(rank, steps=200):
+    """The 48-member ensemble: one captured graph per PERIOD steps (each member
+    a stream branch) against the same members stepped one at a time."""
+    import torch
+    from sles.graph import Ensemble
+    a, b = ensemble_members(rank), ensemble_members(rank)
+    pts = sum(float(d.N) ** d.dim for d in a)
+    ens = Ensemble(a)
+    ens.advance(4)  # capture
+    seq = Ensemble(b)
+    seq.advance_sequential(4)
+    st = torch.cuda.current_stream()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    e[0].record(st)
+    ens.advance(steps)
+    e[1].record(st)
+    seq.advance_sequential(steps)
+    e[2].record(st)
+    torch.cuda.synchronize()
+    tg, ts = e[0].elapsed_time(e[1]) / 1e3, e[1].elapsed_time(e[2]) / 1e3
+    diffs = [rel_l2(x.U_hat, y.U_hat) for x, y in zip(a, b)]
+    out = {"value": round(pts * steps / tg / 1e6, 2), "unit": UNIT, "members": len(a), "steps": steps,
+           "points_per_step": pts, "sequential_value": round(pts * steps / ts / 1e6, 2),
+           "speedup_vs_sequential": round(ts / tg, 3), "max_member_rel_l2_vs_sequential": max(diffs),
+           "config": "32 2D vorticity (N in {256,512,1024}, RK4) + 16 3D Smagorinsky (N in {64,96,128}, RK4), FP32; "
+                     "graph replay with one stream branch per member vs members one at a time"}
+    del a, b, ens, seq
+    torch.cuda.empty_cache()
+    return out
 
 
 def main():
@@ -386,7 +597,14 @@ def main():
                        "speedup_vs_torch_fp64": round(value / world / vtp, 2),
                        "rel_l2_fp32_vs_fp64": err, "steps_compared": kc + 2,
                        "note": "FP32 fused vs FP64 fused (same kernels, float64) on the same seeded field"}
-    out["adjoint_fwd_ratio"] = None
+    if not args.no_compare and world == 1:
+        out["n512"] = bench_512(peak, rank)
+        adj = bench_adjoint(rank)
+        out["adjoint"] = adj
+        out["adjoint_fwd_ratio"] = adj["adjoint_fwd_ratio"]
+        out["ensemble"] = bench_ensemble(rank)
+    else:
+        out["adjoint_fwd_ratio"] = None
 
     # ---------------- CPU baseline (oracle port, bounded sample) ----------------
     if rank == 0 and not args.no_cpu_baseline and world == 1:

@@ -191,6 +191,42 @@ int sles_profile_rhs(sles_plan* plan, const void* u_hat, void* du_scratch, int i
 int sles_rhs_static_workspace(sles_plan* plan, const void* u_hat, const void* u_phys, const void* curl_phys,
                               void* du_out, void* f1_out, void* stream);
 
+/*
+ * Discrete adjoint of the RK4 step (3D; no counterpart in the reference): the
+ * exact transpose of the arithmetic of sles_stage with SLES_STAGE_RK4, i.e. of
+ * computeRHS (src/RK4_method.py:38-71) with u x omega (src/math_formula.py:5-13),
+ * the projection and mask (:52-57), residue_stress (src/math_formula.py:64-127)
+ * with Smagorinsky (src/smagorinsky.py:24-47) or Vreman (src/vreman.py:30-123,
+ * gate held fixed) eddy viscosity, the viscous and forcing terms, and the RK4
+ * combination (src/RK4_method.py:20-35).  Gradients use the real inner product
+ * <x, y> = Re sum conj(x) y over the stored half-complex entries (torch's
+ * convention for complex tensors).  The calls need their own caller-owned
+ * workspace (256-byte aligned, >= sles_adjoint_workspace_bytes, header word
+ * zeroed before first use); the plan's workspace is not touched.
+ *
+ * Reverse sweep over one step whose forward stage s evaluated the RHS at the
+ * state U_s (U_0 = step input, U_1 = U_0 + dt/2 k_0, U_2 = U_0 + dt/2 k_1,
+ * U_3 = U_0 + dt k_2), given ubar = gradient w.r.t. the step output:
+ *   sles_adjoint_seed   acc = ubar, lam = (dt/6) ubar            (once, at the end of time)
+ *   sles_adjoint_prime  prepare the workspace for the stage evaluated at u_state
+ *                       with cotangent lam (needed after a seed, or after a
+ *                       stage called with u_next = NULL)
+ *   sles_adjoint_stage  stage = 3, 2, 1, 0: g = J(U_s)^T lam; acc += g; then
+ *                       lam <- dt/3 ubar + dt g (s=3), dt/3 ubar + dt/2 g (s=2),
+ *                       dt/6 ubar + dt/2 g (s=1); at s=0 ubar <- acc (the
+ *                       gradient w.r.t. the step input) and lam <- (dt/6) acc,
+ *                       which seeds the previous step.  u_next = the state of the
+ *                       next reverse stage (U_{s-1}, or U_3 of the previous
+ *                       step), NULL to skip preparing it.  cs_grad (device
+ *                       double, LES plans) accumulates dL/dCs.
+ * All three field arguments hold 3 half-complex fields of the plan's layout.
+ */
+size_t sles_adjoint_workspace_bytes(const sles_plan* plan);
+int sles_adjoint_seed(sles_plan* plan, void* adj_ws, double dt, const void* ubar, void* acc, void* lam,
+                      void* stream);
+int sles_adjoint_prime(sles_plan* plan, void* adj_ws, const void* u_state, const void* lam, void* stream);
+int sles_adjoint_stage(sles_plan* plan, void* adj_ws, int stage, double dt, const void* u_next, void* ubar,
+                       void* acc, void* lam, double* cs_grad, void* stream);
 /* Human-readable text for a status code (static storage). */
 const char* sles_status_string(int status);
 int sles_version(void);

@@ -513,7 +513,7 @@ def gaussian_vorticity_2d(n, seed=0, kp=10.0):
     nyq = (np.abs(K[0]) == n // 2) | (np.abs(K[1]) == n // 2)
     wh[nyq] = 0.0
     wh[0, 0] = 0.0
-    w = np.fft.irfftn(wh, s=(n, n))
+    w = np.fft.irfftn(wh, s=(n, n), axes=(0, 1))
     w -= w.mean()
     return w / np.sqrt(np.mean(w * w))
 

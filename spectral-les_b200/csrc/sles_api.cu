@@ -185,6 +185,49 @@ int sles_profile_rhs(sles_plan* p, const void* uh, void* du, int iters, double* 
   return p->eng->profile_rhs(p->info, uh, du, iters, ms, (cudaStream_t)stream);
 }
 
+size_t sles_adjoint_workspace_bytes(const sles_plan* p) {
+  if (!p || p->info.d.dim != 3) return 0;
+  const sles::PlanInfo& I = p->info;
+  return sles::slots_offset(I.d.dim, I.d.n) + (size_t)p->eng->adjoint_fields() * I.hc_elems * I.elem_bytes;
+}
+
+// the plan's descriptor with the adjoint workspace in place of its own
+static int adjoint_info(sles_plan* p, void* adj_ws, sles::PlanInfo* out) {
+  if (!p || !adj_ws) return SLES_ERR_INVALID_ARG;
+  if (p->info.d.dim != 3) return SLES_ERR_UNSUPPORTED;
+  if (((uintptr_t)adj_ws) % 256 != 0) return SLES_ERR_INVALID_ARG;
+  *out = p->info;
+  out->ws = adj_ws;
+  out->ws_bytes = sles_adjoint_workspace_bytes(p);
+  out->ws_fields = p->eng->adjoint_fields();
+  out->flags = reinterpret_cast<unsigned*>(adj_ws);
+  out->scal = reinterpret_cast<double*>(reinterpret_cast<char*>(adj_ws) + 256);
+  return SLES_OK;
+}
+
+int sles_adjoint_seed(sles_plan* p, void* adj_ws, double dt, const void* ubar, void* acc, void* lam, void* stream) {
+  sles::PlanInfo I;
+  if (int s = adjoint_info(p, adj_ws, &I)) return s;
+  if (!ubar || !acc || !lam || !(dt == dt)) return SLES_ERR_INVALID_ARG;
+  return p->eng->adjoint_seed(I, dt, ubar, acc, lam, (cudaStream_t)stream);
+}
+
+int sles_adjoint_prime(sles_plan* p, void* adj_ws, const void* u_state, const void* lam, void* stream) {
+  sles::PlanInfo I;
+  if (int s = adjoint_info(p, adj_ws, &I)) return s;
+  if (!u_state || !lam) return SLES_ERR_INVALID_ARG;
+  return p->eng->adjoint_prime(I, u_state, lam, (cudaStream_t)stream);
+}
+
+int sles_adjoint_stage(sles_plan* p, void* adj_ws, int stage, double dt, const void* u_next, void* ubar, void* acc,
+                       void* lam, double* cs_grad, void* stream) {
+  sles::PlanInfo I;
+  if (int s = adjoint_info(p, adj_ws, &I)) return s;
+  if (!ubar || !acc || !lam || !(dt == dt) || stage < 0 || stage > 3) return SLES_ERR_INVALID_ARG;
+  if (p->info.d.les_model != SLES_LES_NONE && !cs_grad) return SLES_ERR_INVALID_ARG;
+  return p->eng->adjoint_stage(I, stage, dt, u_next, ubar, acc, lam, cs_grad, (cudaStream_t)stream);
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

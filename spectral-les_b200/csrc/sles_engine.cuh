@@ -12,6 +12,7 @@
 #include "sles_misc.cuh"
 #include "sles_passes.cuh"
 #include "sles_rhs.cuh"
+#include "sles_adjoint.cuh"
 
 namespace sles {
 
@@ -51,6 +52,12 @@ struct Engine {
   virtual int diag(PlanInfo& p, const void* uh, const void* uphys, double* out, double* spec, int nshell,
                    cudaStream_t st) = 0;
   virtual int profile_rhs(PlanInfo& p, const void* uh, void* du, int iters, double* ms, cudaStream_t st) = 0;
+  // discrete adjoint (3D): workspace slots, seed, prime, one reverse RK4 stage
+  virtual int adjoint_fields() const = 0;
+  virtual int adjoint_seed(PlanInfo& pa, double dt, const void* ubar, void* acc, void* lam, cudaStream_t st) = 0;
+  virtual int adjoint_prime(PlanInfo& pa, const void* u_state, const void* lam, cudaStream_t st) = 0;
+  virtual int adjoint_stage(PlanInfo& pa, int s, double dt, const void* unext, void* ubar, void* acc, void* lam,
+                            double* csgrad, cudaStream_t st) = 0;
 };
 
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? SLES_OK : SLES_ERR_CUDA; }
@@ -520,6 +527,118 @@ struct EngineImpl final : Engine {
     for (int i = 0; i < 6; ++i) cudaEventDestroy(ev[i]);
     for (int k = 0; k < 5; ++k) ms[k] = iters > 0 ? acc[k] / iters : 0.0;
     return status;
+  }
+
+  // ---------------- discrete adjoint (sles_adjoint.cuh) ----------------
+  static constexpr int ADJ_FIELDS = 18;
+  // lines per AZ work item: halved (keeping whole warps) when the staging
+  // buffers and 24 line regions would not fit in shared memory
+  static constexpr int ALPI = (AZGeo<Tp, N, LPI>::SMEM > 227 * 1024 && LPI > 1) ? LPI / 2 : LPI;
+  int adjoint_fields() const override { return DIM == 3 ? ADJ_FIELDS : 0; }
+
+  AXArgs<Tp> axbase(const PlanInfo& pa) const {
+    AXArgs<Tp> a{};
+    a.err = pa.flags;
+    a.ws = slot(pa, 0);
+    a.fs = pa.hc_elems;
+    a.nkp = pa.nkp;
+    a.nk = pa.nk;
+    a.nchunks = nchunks(pa);
+    a.nu = (Tp)pa.d.nu;
+    a.forcing = (Tp)pa.d.forcing;
+    a.kmax = 2.0 / 3.0 * (double)(N / 2 + 1);  // initialize_domain.py:79
+    return a;
+  }
+  int axpass(const PlanInfo& pa, const AXArgs<Tp>& a, cudaStream_t st) {
+    using K = XGeo<Tp, N, FX, 3>;
+    const long long items = (long long)N * nchunks(pa);
+    return launch_persistent(k_adj_xpass<Tp, N, FX>, items, K::THREADS, K::SMEM, st, a);
+  }
+  template <int MODEL>
+  int azpass(const PlanInfo& pa, double* csgrad, cudaStream_t st) {
+    using K = AZGeo<Tp, N, ALPI>;
+    static_assert(K::THREADS % 32 == 0, "whole warps");
+    if (K::SMEM > 227 * 1024) return SLES_ERR_UNSUPPORTED;
+    if (pa.nkp != K::NKP) return SLES_ERR_INVALID_ARG;
+    AZArgs<Tp> a{};
+    a.ws = slot(pa, 0);
+    a.fs = pa.hc_elems;
+    a.nkp = pa.nkp;
+    a.nlines = (long long)N * N;
+    a.scale = (Tp)(1.0 / ((double)N * N * N));
+    const double dx = 2.0 * 3.141592653589793 / N;  // initialize_domain.py:42
+    const double cs = pa.d.cs;
+    a.cdx2 = (MODEL == M_SMAG) ? (Tp)((cs * dx) * (cs * dx)) : (Tp)(2.5 * cs * cs * dx * dx);
+    a.csfac = cs != 0.0 ? 2.0 / cs : 0.0;
+    a.csgrad = csgrad;
+    a.err = pa.flags;
+    return launch_persistent(k_adj_zpass<Tp, N, MODEL, ALPI>, (a.nlines + ALPI - 1) / ALPI, K::THREADS, K::SMEM, st,
+                             a);
+  }
+  int aypass(const PlanInfo& pa, int inv, cudaStream_t st) {
+    using K = TGeo<Tp, N, FY>;
+    YArgs<Tp> a{};
+    const long long cb = sizeof(C);
+    SLES_TRY(make_tmap(&a.tm, slot(pa, 0), K::EPC, pa.nk, N, (long long)pa.nkp * cb, N, (long long)N * pa.nkp * cb,
+                       pa.ws_fields, pa.hc_elems * cb, K::W, K::RB));
+    a.err = pa.flags;
+    a.ws = slot(pa, 0);
+    a.fs = pa.hc_elems;
+    a.nkp = pa.nkp;
+    a.nk = pa.nk;
+    a.nchunks = nchunks(pa);
+    const long long items = (long long)N * nchunks(pa);
+    if (inv) return launch_persistent(k_ypass<Tp, N, FY, 1, 1, 1>, items, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_ypass<Tp, N, FY, 1, 0, 1>, items, K::THREADS, K::SMEM, st, a);
+  }
+
+  int adjoint_seed(PlanInfo& pa, double dt, const void* ubar, void* acc, void* lam, cudaStream_t st) override {
+    if (DIM != 3) return SLES_ERR_UNSUPPORTED;
+    return launch(k_adj_seed<Tp>, 1184, 256, 0, st, (const C*)ubar, (C*)acc, (C*)lam, 3 * pa.hc_elems,
+                  (Tp)(dt / 6.0));
+  }
+  int adjoint_prime(PlanInfo& pa, const void* u_state, const void* lam, cudaStream_t st) override {
+    if constexpr (DIM != 3) {
+      return SLES_ERR_UNSUPPORTED;
+    } else {
+      if (pa.ws_fields < ADJ_FIELDS) return SLES_ERR_WORKSPACE;
+      AXArgs<Tp> a = axbase(pa);
+      a.fwd = 0;
+      a.prep = 1;
+      a.unext = (const C*)u_state;
+      a.lam = (C*)lam;
+      return axpass(pa, a, st);
+    }
+  }
+  int adjoint_stage(PlanInfo& pa, int s, double dt, const void* unext, void* ubar, void* acc, void* lam,
+                    double* csgrad, cudaStream_t st) override {
+    if constexpr (DIM != 3) {
+      return SLES_ERR_UNSUPPORTED;
+    } else {
+      if (pa.ws_fields < ADJ_FIELDS) return SLES_ERR_WORKSPACE;
+      if (s < 0 || s > 3) return SLES_ERR_INVALID_ARG;
+      SLES_TRY(aypass(pa, 1, st));
+      switch (pa.d.les_model) {
+        case SLES_LES_SMAGORINSKY: SLES_TRY(azpass<M_SMAG>(pa, csgrad, st)); break;
+        case SLES_LES_VREMAN: SLES_TRY(azpass<M_VREMAN>(pa, csgrad, st)); break;
+        default: SLES_TRY(azpass<M_NONE>(pa, csgrad, st)); break;
+      }
+      SLES_TRY(aypass(pa, 0, st));
+      AXArgs<Tp> a = axbase(pa);
+      a.fwd = 1;
+      a.prep = unext ? 1 : 0;
+      a.unext = (const C*)unext;
+      a.ubar = (C*)ubar;
+      a.acc = (C*)acc;
+      a.lam = (C*)lam;
+      // reverse RK4 stage s: lam <- alpha ubar + beta g;  s = 0: ubar <- acc, lam <- dt/6 acc
+      static const double al[4] = {1.0 / 6.0, 1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0};
+      static const double be[4] = {0.0, 0.5, 0.5, 1.0};
+      a.alpha = (Tp)(al[s] * dt);
+      a.beta = (Tp)(be[s] * dt);
+      a.last = (s == 0) ? 1 : 0;
+      return axpass(pa, a, st);
+    }
   }
 
   int diag(PlanInfo& p, const void* uh, const void* uphys, double* out, double* spec, int nshell,

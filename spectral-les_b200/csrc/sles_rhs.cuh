@@ -224,6 +224,10 @@ __device__ __forceinline__ int seq_slot(int i) {
   if (KIND == 1) { const int s[5] = {2, 0, 4, 1, 3}; return s[i]; }
   if (KIND == 2) { const int s[9] = {4, 5, 0, 3, 6, 7, 1, 8, 2}; return s[i]; }
   if (KIND == 4) { const int s[6] = {0, 3, 1, 4, 2, 5}; return s[i]; }
+  // 6: adjoint y-inverse (two groups of 6 inputs at slot bases 0 and 9),
+  // 7: adjoint y-forward (Z_j, A2_j, A1_j per component)
+  if (KIND == 6) { const int s[6] = {0, 3, 1, 4, 2, 5}; return (i / 6) * 9 + s[i % 6]; }
+  if (KIND == 7) { const int s[9] = {0, 6, 3, 1, 7, 4, 2, 8, 5}; return s[i]; }
   return i;
 }
 
@@ -389,15 +393,18 @@ struct YArgs {
   int nkp, nk, nchunks;
 };
 
-// INV = 1: inverse (y1), 0: forward (y2)
-template <typename Tp, int N, class F, int LES, int INV>
+// INV = 1: inverse (y1), 0: forward (y2).  ADJ = 1: the adjoint's passes
+// (discrete adjoint of the RHS, see sles_adjoint.cuh): the inverse carries two
+// groups (the recomputed state and the cotangent), the forward contracts
+// Z_j - i ky A2_j.
+template <typename Tp, int N, class F, int LES, int INV, int ADJ = 0>
 __global__ void __launch_bounds__(TGeo<Tp, N, F>::THREADS, TGeo<Tp, N, F>::MINB)
 k_ypass(const __grid_constant__ YArgs<Tp> A) {
   using K = TGeo<Tp, N, F>;
   using C = typename CT<Tp>::C;
   constexpr int T = K::T, V = K::V, W = K::W;
-  constexpr int KIND = INV ? (LES ? 0 : 1) : (LES ? 2 : 3);
-  constexpr int NT = INV ? (LES ? 6 : 5) : (LES ? 9 : 3);
+  constexpr int KIND = ADJ ? (INV ? 6 : 7) : (INV ? (LES ? 0 : 1) : (LES ? 2 : 3));
+  constexpr int NT = ADJ ? (INV ? 12 : 9) : (INV ? (LES ? 6 : 5) : (LES ? 9 : 3));
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   typename K::Ring ring;
   const int tid = threadIdx.x;
@@ -447,21 +454,42 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
         for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
       }
     };
+    if (ADJ && !INV) {
+      C v[V], w[V];
+#pragma unroll 1
+      for (int c = 0; c < 3; ++c) {  // Y_c = Y(Z_c) - i ky Y(A2_c);  A1_c passes through
+        take(v);
+        fft.template run_tab<-1>(v, j, sm, W, twt);
+        take(w);
+        fft.template run_tab<-1>(w, j, sm, W, twt);
+#pragma unroll
+        for (int m = 0; m < V; ++m) v[m] = cadd(v[m], cmuli_s(w[m], -kyv(m)));
+        st(c, v);
+        take(v);
+        fft.template run_tab<-1>(v, j, sm, W, twt);
+        st(3 + c, v);
+      }
+      continue;
+    }
     if (INV) {
       C v[V], w[V];
       if (LES) {
 #pragma unroll 1
-        for (int c = 0; c < 3; ++c) {  // a_c, dy_c = Y^-1(i ky A_c), dx_c = Y^-1(B_c)
-          take(v);
+        for (int g = 0; g < (ADJ ? 2 : 1); ++g) {
+          const int sb = 9 * g;
+#pragma unroll 1
+          for (int c = 0; c < 3; ++c) {  // a_c, dy_c = Y^-1(i ky A_c), dx_c = Y^-1(B_c)
+            take(v);
 #pragma unroll
-          for (int m = 0; m < V; ++m) w[m] = cmuli_s(v[m], kyv(m));
-          fft.template run_tab<+1>(v, j, sm, W, twt);
-          st(c, v);
-          fft.template run_tab<+1>(w, j, sm, W, twt);
-          st(6 + c, w);
-          take(v);
-          fft.template run_tab<+1>(v, j, sm, W, twt);
-          st(3 + c, v);
+            for (int m = 0; m < V; ++m) w[m] = cmuli_s(v[m], kyv(m));
+            fft.template run_tab<+1>(v, j, sm, W, twt);
+            st(sb + c, v);
+            fft.template run_tab<+1>(w, j, sm, W, twt);
+            st(sb + 6 + c, w);
+            take(v);
+            fft.template run_tab<+1>(v, j, sm, W, twt);
+            st(sb + 3 + c, v);
+          }
         }
       } else {
         take(v);  // A_w -> a_w and Ox = Y^-1(i ky A_w)

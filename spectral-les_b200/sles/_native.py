@@ -25,6 +25,7 @@ EXPORTED = [
     "sles_plan_set_workspace", "sles_plan_set_params", "sles_fft_r2c", "sles_fft_c2r",
     "sles_velocity_curl", "sles_velocity_gradient", "sles_rhs", "sles_stage", "sles_diag",
     "sles_status_string", "sles_version", "sles_profile_rhs", "sles_rhs_static_workspace",
+    "sles_adjoint_workspace_bytes", "sles_adjoint_seed", "sles_adjoint_prime", "sles_adjoint_stage",
 ]
 
 
@@ -77,6 +78,10 @@ def load_library(path: str = LIB_PATH):
         "sles_profile_rhs": (i, [vp, vp, vp, i, vp, vp]),
         "sles_rhs_static_workspace": (i, [vp, vp, vp, vp, vp, vp, vp]),
         "sles_version": (i, []),
+        "sles_adjoint_workspace_bytes": (ctypes.c_size_t, [vp]),
+        "sles_adjoint_seed": (i, [vp, vp, d, vp, vp, vp, vp]),
+        "sles_adjoint_prime": (i, [vp, vp, vp, vp, vp]),
+        "sles_adjoint_stage": (i, [vp, vp, i, d, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -168,6 +173,29 @@ class Plan:
         check(self.L.sles_profile_rhs(self.h, ptr(uh), ptr(du), int(iters), ms, stream_handle(self.device)),
               "sles_profile_rhs")
         return list(ms)
+
+    # discrete adjoint (include/sles.h); ws: the adjoint workspace (uint8 tensor)
+    def adjoint_workspace(self):
+        """A zeroed, 256-byte aligned adjoint workspace: (owner tensor, aligned pointer)."""
+        nbytes = int(self.L.sles_adjoint_workspace_bytes(self.h))
+        if nbytes == 0:
+            raise SlesError(2, "sles_adjoint_workspace_bytes")
+        with torch.cuda.device(self.device):
+            t = torch.zeros(nbytes + 256, dtype=torch.uint8, device=self.device)
+        return t, t.data_ptr() + (-t.data_ptr()) % 256
+
+    def adjoint_seed(self, ws_ptr, dt, ubar, acc, lam):
+        check(self.L.sles_adjoint_seed(self.h, ctypes.c_void_p(ws_ptr), float(dt), ptr(ubar), ptr(acc), ptr(lam),
+                                       stream_handle(self.device)), "sles_adjoint_seed")
+
+    def adjoint_prime(self, ws_ptr, u_state, lam):
+        check(self.L.sles_adjoint_prime(self.h, ctypes.c_void_p(ws_ptr), ptr(u_state), ptr(lam),
+                                        stream_handle(self.device)), "sles_adjoint_prime")
+
+    def adjoint_stage(self, ws_ptr, stage, dt, u_next, ubar, acc, lam, cs_grad):
+        check(self.L.sles_adjoint_stage(self.h, ctypes.c_void_p(ws_ptr), int(stage), float(dt), ptr(u_next),
+                                        ptr(ubar), ptr(acc), ptr(lam), ptr(cs_grad), stream_handle(self.device)),
+              "sles_adjoint_stage")
 
     def diag(self, uh, out, uphys=None, spectrum=None):
         ns = 0 if spectrum is None else spectrum.numel()

@@ -1,0 +1,201 @@
+"""Differentiable RK4 rollouts: the fused forward steps with a hand-written
+discrete adjoint behind ``torch.autograd.Function`` (3D).
+
+    ro = RK4Rollout(n=128, nu=2e-4, dt=2e-3, les="Smagorinsky", dtype=torch.float32,
+                    checkpoint_every=10)
+    U0 = ro.rfft(u_phys).requires_grad_()          # (3, n, n, n//2+1) complex
+    Cs = torch.tensor(0.17, dtype=torch.float64, requires_grad=True)
+    UT = ro(U0, Cs, nsteps=100)                    # fused RK4 steps (src/RK4_method.py:20-71)
+    loss = log_spectrum_misfit(UT, E_target, n)
+    loss.backward()                                # U0.grad, Cs.grad
+
+The forward keeps the state every ``checkpoint_every`` steps.  The backward
+walks the segments from the last to the first: it recomputes a segment's
+steps from its checkpoint, keeping each step's four stage states, then runs
+the reverse stages (``sles_adjoint_stage``, the transpose of the fused
+right-hand side and of the RK4 combination) through it.  Gradients follow
+torch's convention for complex tensors (dL/dRe + i dL/dIm of every stored
+half-complex entry), so they compare directly with torch.fft autograd.
+"""
+from __future__ import annotations
+
+import math
+
+import torch
+
+from . import _native as nat
+
+__all__ = ["RK4Rollout", "shell_spectrum", "log_spectrum_misfit"]
+
+_SIZES = (16, 24, 32, 48, 64, 96, 128, 256, 512)
+
+
+class RK4Rollout:
+    def __init__(self, n, nu, dt, les="Smagorinsky", Cs=0.17, dtype=torch.float32, parity=True, forcing=0.0,
+                 checkpoint_every=10, device="cuda"):
+        if int(n) not in _SIZES:
+            raise ValueError("grid N=%d is not compiled (supported: %s)" % (n, _SIZES))
+        if checkpoint_every < 1:
+            raise ValueError("checkpoint_every must be >= 1")
+        self.n, self.nu, self.dt = int(n), float(nu), float(dt)
+        self.forcing, self.every = float(forcing), int(checkpoint_every)
+        model = nat.LES_NONE
+        if les is not None:
+            if les[0] not in "SsVv":
+                raise ValueError("LES model must be 'Smagorinsky' or 'vreman'")
+            model = nat.LES_SMAGORINSKY if les[0] in "Ss" else nat.LES_VREMAN
+        self.les = model
+        self.Cs = float(Cs)
+        self.rdtype = dtype
+        self.cdtype = torch.complex64 if dtype == torch.float32 else torch.complex128
+        self.device = torch.device(device)
+        self.plan = nat.Plan(3, self.n, dtype, model, nat.SCHEME_RK4, parity, nu, Cs, forcing, self.device)
+        self.nk, self.nkp = self.plan.nk, self.plan.nkp
+        self._ws_owner, self._ws = self.plan.adjoint_workspace()
+        self._store = []   # stage states of the segment being reversed (reused across calls)
+
+    # ---- storage helpers ----
+    def _new(self):
+        return torch.zeros((3, self.n, self.n, self.nkp), dtype=self.cdtype, device=self.device)
+
+    def _pad(self, U):
+        s = self._new()
+        s[..., : self.nk].copy_(U.detach().to(self.cdtype))
+        return s
+
+    def rfft(self, u):
+        """(3, n, n, n) real -> (3, n, n, n//2+1) complex with this rollout's own r2c."""
+        u = torch.as_tensor(u, device=self.device).to(self.rdtype).contiguous()
+        s = self._new()
+        self.plan.fft_r2c(u, s, 3)
+        return s[..., : self.nk].clone()
+
+    # ---- forward ----
+    def _step(self, A, B, Cacc, primed):
+        """One fused RK4 step from A (kept) into B; Cacc is the accumulator
+        (overwritten).  Returns True (the workspace is primed with B)."""
+        Cacc.copy_(A)  # U_hat1 = U_hat at step entry (SM_solver.py:33)
+        for rk in range(4):
+            flags = nat.STAGE_RK4 | (nat.STAGE_PRIMED if (primed and rk == 0) or rk > 0 else 0)
+            self.plan.stage(rk, self.dt, A if rk == 0 else B, A, Cacc, B, None, None, None, flags)
+        return True
+
+    def _step_keep(self, A, stages, Cacc, primed):
+        """As _step, writing the stage states U_1..U_3 to stages[0..2] and the
+        step output to stages[3]."""
+        Cacc.copy_(A)
+        cur = A
+        for rk in range(4):
+            flags = nat.STAGE_RK4 | (nat.STAGE_PRIMED if (primed and rk == 0) or rk > 0 else 0)
+            self.plan.stage(rk, self.dt, cur, A, Cacc, stages[rk], None, None, None, flags)
+            cur = stages[rk]
+        return True
+
+    def forward_states(self, U0, Cs, nsteps):
+        """Run ``nsteps`` fused RK4 steps; return (U_T padded, checkpoints)."""
+        self.plan.set_params(self.nu, Cs, self.forcing)
+        A, B, Cacc = self._pad(U0), self._new(), self._new()
+        ckpts = {0: A.clone()}
+        primed = False
+        for k in range(int(nsteps)):
+            primed = self._step(A, B, Cacc, primed)
+            A, B = B, A
+            if (k + 1) % self.every == 0 and (k + 1) < nsteps:
+                ckpts[k + 1] = A.clone()
+        return A, ckpts
+
+    # ---- backward ----
+    def backward_states(self, ckpts, gUT, Cs, nsteps):
+        """Reverse sweep; returns (dL/dU_0 padded, dL/dCs float64 tensor)."""
+        self.plan.set_params(self.nu, Cs, self.forcing)
+        dt = self.dt
+        ubar, acc, lam = self._pad(gUT), self._new(), self._new()
+        csg = torch.zeros(1, dtype=torch.float64, device=self.device)
+        self.plan.adjoint_seed(self._ws, dt, ubar, acc, lam)
+        starts = sorted(ckpts)
+        ends = starts[1:] + [int(nsteps)]
+        Cacc = self._new()
+        store = self._store
+        while len(store) < max(e - s for s, e in zip(starts, ends)):
+            store.append([self._new() for _ in range(4)])
+        for s0, s1 in reversed(list(zip(starts, ends))):
+            m = s1 - s0
+            # recompute the segment: inputs[i] = state entering step s0 + i
+            inputs = [ckpts[s0]]
+            primed = False
+            for i in range(m):
+                primed = self._step_keep(inputs[i], store[i], Cacc, primed)
+                inputs.append(store[i][3])
+            # stage states of step i: U_0 = inputs[i], U_1..U_3 = store[i][0..2]
+            states = lambda i, s: inputs[i] if s == 0 else store[i][s - 1]
+            self.plan.adjoint_prime(self._ws, states(m - 1, 3), lam)
+            for i in range(m - 1, -1, -1):
+                for s in (3, 2, 1, 0):
+                    if s > 0:
+                        un = states(i, s - 1)
+                    else:
+                        un = states(i - 1, 3) if i > 0 else None
+                    self.plan.adjoint_stage(self._ws, s, dt, un, ubar, acc, lam, csg)
+        return ubar, csg
+
+    def __call__(self, U0, Cs, nsteps):
+        if not torch.is_tensor(Cs):
+            Cs = torch.tensor(float(Cs), dtype=torch.float64, device=self.device)
+        return _RolloutFn.apply(U0, Cs, self, int(nsteps))
+
+    def timed(self, U0, Cs, nsteps, gUT):
+        """(forward ms, backward ms, U_T, dL/dU_0, dL/dCs) of one rollout and its
+        reverse sweep, timed with CUDA events on the current stream."""
+        st = torch.cuda.current_stream(self.device)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize(self.device)
+        e[0].record(st)
+        UT, ck = self.forward_states(U0, float(Cs), nsteps)
+        e[1].record(st)
+        g, c = self.backward_states(ck, gUT, float(Cs), nsteps)
+        e[2].record(st)
+        torch.cuda.synchronize(self.device)
+        return e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), UT, g, c
+
+
+class _RolloutFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, U0, Cs, ro, nsteps):
+        UT, ckpts = ro.forward_states(U0, float(Cs), nsteps)
+        ctx.ro, ctx.ckpts, ctx.nsteps, ctx.cs = ro, ckpts, nsteps, float(Cs)
+        ctx.u_dtype, ctx.cs_dtype = U0.dtype, Cs.dtype
+        return UT[..., : ro.nk].clone()
+
+    @staticmethod
+    def backward(ctx, gUT):
+        ro = ctx.ro
+        g, csg = ro.backward_states(ctx.ckpts, gUT.contiguous(), ctx.cs, ctx.nsteps)
+        ctx.ckpts = None
+        gU = g[..., : ro.nk].clone().to(ctx.u_dtype)
+        return gU, csg[0].to(ctx.cs_dtype), None, None
+
+
+def shell_spectrum(U_hat, n, nshells=None):
+    """E(k) on integer shells round(|k|): 1/2 sum w |u_hat|^2 / N^6, w = 2 on
+    0 < kz < N/2, in float64 (differentiable torch ops)."""
+    dev = U_hat.device
+    kc = (torch.fft.fftfreq(n, device=dev, dtype=torch.float64) * n).round()
+    kz = torch.arange(n // 2 + 1, device=dev, dtype=torch.float64)
+    K2 = kc.view(n, 1, 1) ** 2 + kc.view(1, n, 1) ** 2 + kz.view(1, 1, -1) ** 2
+    w = torch.where((kz > 0) & (kz < n // 2), 2.0, 1.0).view(1, 1, -1)
+    rd = torch.float64  # accumulated in float64 whatever the state's precision
+    ur, ui = U_hat.real.to(rd), U_hat.imag.to(rd)
+    e = 0.5 * w * (ur * ur + ui * ui).sum(0) / float(n) ** 6
+    shell = torch.round(torch.sqrt(K2)).long().reshape(-1)
+    ns = int(shell.max()) + 1 if nshells is None else int(nshells)
+    keep = shell < ns
+    return torch.zeros(ns, dtype=rd, device=dev).index_add(0, shell[keep], e.reshape(-1)[keep])
+
+
+def log_spectrum_misfit(U_hat, E_target, n, kmin=1, kmax=None):
+    """sum_{k=kmin..kmax} (log E(k) - log E_target(k))^2, kmax = floor(2/3 (N/2+1))."""
+    kmax = int(math.floor(2.0 / 3.0 * (n // 2 + 1))) if kmax is None else int(kmax)
+    E = shell_spectrum(U_hat, n, kmax + 1)
+    Et = torch.as_tensor(E_target, device=U_hat.device)[: kmax + 1].to(E.dtype)
+    d = torch.log(E[kmin: kmax + 1]) - torch.log(Et[kmin: kmax + 1])
+    return (d * d).sum()

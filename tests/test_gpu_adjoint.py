@@ -1,0 +1,126 @@
+"""The hand-written discrete adjoint of the fused RK4 rollout.
+
+Checked three ways: against torch.fft autograd through the plain torch path
+(float64, same arithmetic up to rounding), against central finite differences
+of the fused forward (float64), and float32 against float64 at the adjoint
+configuration's full size (128^3, 100 steps, checkpoints every 10).
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from sles.adjoint import RK4Rollout, log_spectrum_misfit, shell_spectrum
+from sles.plain_torch import PlainSolver
+from sles.synthetic import random_spectrum_velocity
+
+pytestmark = pytest.mark.gpu
+
+
+def _field(n, seed=3, k0=4.0):
+    u, v, w = random_spectrum_velocity(n, k0, 1.0, seed=seed)
+    return torch.stack([torch.as_tensor(x) for x in (u, v, w)]).to("cuda", torch.float64)
+
+
+def _rel(a, b):
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+
+@pytest.mark.parametrize("les", ["Smagorinsky", "vreman", None])
+def test_one_step_vjp_matches_torch_autograd(les):
+    n, nu, dt, cs = 32, 3e-3, 5e-3, 0.17
+    ro = RK4Rollout(n, nu, dt, les=les, Cs=cs, dtype=torch.float64, checkpoint_every=1)
+    ps = PlainSolver(n, 3, nu=nu, dt=dt, les=les, Cs=cs, method="RK4", device="cuda")
+    U0 = ps.rfft(_field(n))
+    g = torch.Generator(device="cuda").manual_seed(1)
+    lam = torch.complex(torch.randn(U0.shape, generator=g, device="cuda", dtype=torch.float64),
+                        torch.randn(U0.shape, generator=g, device="cuda", dtype=torch.float64))
+    # torch autograd through the plain path
+    Ua = U0.clone().requires_grad_(True)
+    Ca = torch.tensor(cs, dtype=torch.float64, device="cuda", requires_grad=True)
+    La = (torch.conj(lam) * ps.rk4(Ua, Ca)).real.sum()
+    gU_ref, = torch.autograd.grad(La, [Ua], retain_graph=True)
+    gC_ref = torch.autograd.grad(La, [Ca])[0] if les else None
+    # the fused path and its adjoint
+    Ub = U0.clone().requires_grad_(True)
+    Cb = torch.tensor(cs, dtype=torch.float64, device="cuda", requires_grad=True)
+    UT = ro(Ub, Cb, 1)
+    assert _rel(UT.detach(), ps.rk4(U0).detach()) < 1e-12
+    Lb = (torch.conj(lam) * UT).real.sum()
+    Lb.backward()
+    assert _rel(Ub.grad, gU_ref) < 1e-10
+    if les:
+        assert abs(float(Cb.grad) - float(gC_ref)) <= 1e-9 * abs(float(gC_ref))
+
+
+def test_checkpointed_rollout_matches_torch_autograd():
+    n, nu, dt, cs, steps = 32, 2e-3, 5e-3, 0.17, 7
+    ro = RK4Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=torch.float64, checkpoint_every=3)
+    ps = PlainSolver(n, 3, nu=nu, dt=dt, les="Smagorinsky", Cs=cs, method="RK4", device="cuda")
+    U0 = ps.rfft(_field(n, seed=4))
+    Et = shell_spectrum(U0, n).detach() * 0.9
+    Ua = U0.clone().requires_grad_(True)
+    Ca = torch.tensor(cs, dtype=torch.float64, device="cuda", requires_grad=True)
+    La = log_spectrum_misfit(ps.rollout(Ua, steps, Ca), Et, n)
+    La.backward()
+    Ub = U0.clone().requires_grad_(True)
+    Cb = torch.tensor(cs, dtype=torch.float64, device="cuda", requires_grad=True)
+    Lb = log_spectrum_misfit(ro(Ub, Cb, steps), Et, n)
+    Lb.backward()
+    assert abs(float(La.detach()) - float(Lb.detach())) <= 1e-11 * abs(float(La.detach()))
+    assert _rel(Ub.grad, Ua.grad) < 1e-9
+    assert abs(float(Cb.grad) - float(Ca.grad)) <= 1e-9 * abs(float(Ca.grad))
+
+
+def _loss(ro, U0, cs, steps, Et, n):
+    with torch.no_grad():
+        return float(log_spectrum_misfit(ro(U0, torch.tensor(cs, dtype=torch.float64, device="cuda"), steps),
+                                         Et, n))
+
+
+@pytest.mark.parametrize("les", ["Smagorinsky", "vreman"])
+def test_gradients_match_central_differences(les):
+    n, nu, dt, cs, steps = 48, 2e-4, 2e-3, 0.17, 12
+    ro = RK4Rollout(n, nu, dt, les=les, Cs=cs, dtype=torch.float64, checkpoint_every=5)
+    U0 = ro.rfft(_field(n, seed=6))
+    Et = shell_spectrum(U0, n).detach() * torch.linspace(0.8, 1.2, shell_spectrum(U0, n).numel(), device="cuda",
+                                                         dtype=torch.float64)
+    U = U0.clone().requires_grad_(True)
+    C = torch.tensor(cs, dtype=torch.float64, device="cuda", requires_grad=True)
+    log_spectrum_misfit(ro(U, C, steps), Et, n).backward()
+    # C_s: central differences with eps = 1e-3 and 5e-4; their truncation error
+    # is O(eps^2) (~1e-4 relative here), the Richardson combination's O(eps^4)
+    cd = lambda e: (_loss(ro, U0, cs + e, steps, Et, n) - _loss(ro, U0, cs - e, steps, Et, n)) / (2 * e)
+    fd1, fd2 = cd(1e-3), cd(5e-4)
+    rich = (4.0 * fd2 - fd1) / 3.0
+    assert abs(rich - float(C.grad)) <= 1e-5 * abs(rich)
+    assert abs(fd1 - float(C.grad)) <= 1e-3 * abs(fd1)
+    # U_hat: random-direction probes (a solenoidal, real-consistent direction)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    for _ in range(2):
+        d = ro.rfft(_field(n, seed=int(torch.randint(100, 1000, (1,), generator=g, device="cuda"))))
+        d = d / torch.linalg.vector_norm(d) * torch.linalg.vector_norm(U0)
+        h = 1e-5
+        fd = (_loss(ro, U0 + h * d, cs, steps, Et, n) - _loss(ro, U0 - h * d, cs, steps, Et, n)) / (2 * h)
+        an = float((torch.conj(U.grad) * d).real.sum())
+        assert abs(fd - an) <= 1e-5 * abs(fd)
+
+
+def test_adjoint_configuration_float32_against_float64():
+    """128^3 Smagorinsky, RK4, nu=2e-4, dt=2e-3, 100 steps, checkpoints every 10:
+    float32 gradients against float64 gradients of the same fused path."""
+    n, nu, dt, cs, steps = 128, 2e-4, 2e-3, 0.17, 100
+    r64 = RK4Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=torch.float64, checkpoint_every=10)
+    r32 = RK4Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=torch.float32, checkpoint_every=10)
+    U0 = r64.rfft(_field(n, seed=0))
+    Et = shell_spectrum(U0, n).detach() * 0.8
+    grads = []
+    for ro, dtp in ((r64, torch.complex128), (r32, torch.complex64)):
+        U = U0.to(dtp).clone().requires_grad_(True)
+        C = torch.tensor(cs, dtype=torch.float64, device="cuda", requires_grad=True)
+        log_spectrum_misfit(ro(U, C, steps), Et, n, kmax=20).backward()
+        grads.append((U.grad.to(torch.complex128), float(C.grad)))
+    (g64, c64), (g32, c32) = grads
+    assert _rel(g32, g64) < 1e-3
+    assert abs(c32 - c64) <= 1e-3 * abs(c64)
