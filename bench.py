@@ -146,12 +146,35 @@ def make_domain(n, dtype, seed, method="RK3", les="Smagorinsky", nu=NU, cs=CS, d
     return d
 
 
-def spectrum_error(a, b, n):
-    """max_k |E_a(k) - E_b(k)| / E_b(k) over integer shells 1..floor(2/3 (N/2+1))."""
+def spectrum_error(a, b, n, floor=1e-8):
+    """E(k) error of a against b on integer shells 1..floor(2/3 (N/2+1)):
+    (max relative error over the shells holding at least ``floor`` of the peak
+    shell energy, the last such shell, max relative error over all shells).
+    Shells far below the peak carry round-off-level energy in float32, where
+    the relative error measures the float32 noise floor, not the dynamics."""
     from sles.adjoint import shell_spectrum
     kc = int(2.0 / 3.0 * (n // 2 + 1))
     ea, eb = shell_spectrum(a, n, kc + 1)[1:], shell_spectrum(b, n, kc + 1)[1:]
-    return float(((ea - eb).abs() / eb).max())
+    r = (ea - eb).abs() / eb
+    live = eb >= floor * eb.max()
+    klast = int(torch_nonzero_last(live)) + 1
+    return float(r[live].max()), klast, float(r.max())
+
+
+def torch_nonzero_last(mask):
+    return mask.nonzero().max()
+
+
+def tune_domain(d):
+    """Run the autotuner on a domain (outside any timed region); the cache goes
+    to a per-process temporary file unless SLES_TUNE_CACHE is set."""
+    import tempfile
+    from sles import autotune
+    if not os.environ.get("SLES_TUNE_CACHE"):
+        os.environ["SLES_TUNE_CACHE"] = os.path.join(tempfile.gettempdir(), "sles_bench_tune_%d.json" % os.getpid())
+    times = autotune.tune(d)
+    return {"x_pass_variant": d._plan.get_variant(0), "ms_per_step_by_variant": {str(k): round(v, 4)
+                                                                                  for k, v in times.items()}}
 
 
 def rel_l2(a, b):
@@ -172,6 +195,7 @@ def bench_512(peak, rank):
     # -- Smagorinsky RK3 at 512^3
     d32 = make_domain(n, "float32", rank)
     d64 = make_domain(n, "float64", rank)
+    tu = [tune_domain(d32), tune_domain(d64)]
     for _ in range(3):
         step(d32)
         step(d64)
@@ -181,7 +205,7 @@ def bench_512(peak, rank):
         step(d32)
         step(d64)
     err = rel_l2(d32.U_hat, d64.U_hat)
-    ek = spectrum_error(d32.U_hat, d64.U_hat, n)
+    ek, klive, ekall = spectrum_error(d32.U_hat, d64.U_hat, n)
     kms = d32._plan.profile_rhs(d32._s_uhat, d32._new_hc(3), 10)
     del d32, d64
     torch.cuda.empty_cache()
@@ -193,10 +217,13 @@ def bench_512(peak, rank):
         "value": round(v32, 2), "unit": UNIT, "ms_per_step": round(ms, 3),
         "fused_fp64_value": round(v64, 2), "torch_fft_fp64_value": round(vtp, 2),
         "speedup_vs_torch_fp64": round(v32 / vtp, 2), "speedup_vs_fused_fp64": round(v32 / v64, 2),
-        "rel_l2_fp32_vs_fp64_after_100_steps": err, "ek_err_fp32_vs_fp64_after_100_steps": ek,
+        "rel_l2_fp32_vs_fp64_after_100_steps": err,
+        "ek_err_fp32_vs_fp64_after_100_steps": {"max_rel_shells_above_1e-8_of_peak": ek, "up_to_shell": klive,
+                                                "max_rel_all_shells": ekall},
         "step_roofline_frac": round(STEP_BYTES_PER_PT_RHS["f32"] * 3 * npts / (ms * 1e-3) / 1e9 / peak, 4),
         "kernel_ms": dict(zip(["x_inverse", "y_inverse", "z_fused", "y_forward", "x_forward_combine"],
                               [round(x, 4) for x in kms])),
+        "autotune_fp32_fp64": tu,
         "config": "512^3, random-phase spectrum k0=4, nu=1e-4, Smagorinsky Cs=0.17, reference RK3, dt=1e-3"}
     # -- Vreman ETD2 at 512^3
     cs_v = math.sqrt(0.07 / 2.5)
@@ -204,6 +231,7 @@ def bench_512(peak, rank):
                                  parity=False)
     estep = ETD2_method.solveForNextTimestep
     d32, d64 = mk("float32"), mk("float64")
+    tu = [tune_domain(d32), tune_domain(d64)]
     for _ in range(3):
         estep(d32)
         estep(d64)
@@ -213,7 +241,7 @@ def bench_512(peak, rank):
         estep(d32)
         estep(d64)
     err = rel_l2(d32.U_hat, d64.U_hat)
-    ek = spectrum_error(d32.U_hat, d64.U_hat, n)
+    ek, klive, ekall = spectrum_error(d32.U_hat, d64.U_hat, n)
     kms = d32._plan.profile_rhs(d32._s_uhat, d32._new_hc(3), 10)
     fbytes = float(n) * n * (n // 2 + 1) * 8
     algb = {"x_inverse": 9 * fbytes, "y_inverse": 15 * fbytes, "z_fused": 18 * fbytes, "y_forward": 15 * fbytes,
@@ -225,10 +253,13 @@ def bench_512(peak, rank):
     out["vreman_etd2"] = {
         "value": round(npts * 20 / t32 / 1e6, 2), "unit": UNIT, "ms_per_step": round(ms, 3),
         "fused_fp64_value": round(npts * 20 / t64 / 1e6, 2),
-        "rel_l2_fp32_vs_fp64_after_100_steps": err, "ek_err_fp32_vs_fp64_after_100_steps": ek,
+        "rel_l2_fp32_vs_fp64_after_100_steps": err,
+        "ek_err_fp32_vs_fp64_after_100_steps": {"max_rel_shells_above_1e-8_of_peak": ek, "up_to_shell": klive,
+                                                "max_rel_all_shells": ekall},
         "step_roofline_frac": round(STEP_BYTES_PER_PT_RHS["f32"] * 1 * npts / (ms * 1e-3) / 1e9 / peak, 4),
         "kernel_ms": dict(zip(names, [round(x, 4) for x in kms])),
         "kernel_gbs": {k: round(algb[k] / (t * 1e-3) / 1e9, 1) for k, t in zip(names, kms)},
+        "autotune_fp32_fp64": tu,
         "config": "512^3, random-phase spectrum k0=6, nu=5e-5, Vreman c=0.07 (Cs=%.5f), ETD2 (Cox-Matthews, "
                   "float64 phi coefficients), dt=5e-4" % cs_v}
     return out
@@ -361,7 +392,11 @@ def bench_adjoint(rank):
     del dT
     d0 = make_domain(n, "float64", rank, method="RK4", nu=nu, dt=dt)
     U0 = d0.U_hat.clone()
+    tune_domain(d0)
     del d0
+    d1 = make_domain(n, "float32", rank, method="RK4", nu=nu, dt=dt)
+    tune_domain(d1)
+    del d1
     res = {}
     for name, dtp in (("f32", torch.float32), ("f64", torch.float64)):
         ro = RK4Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=dtp, checkpoint_every=10)
@@ -377,7 +412,7 @@ def bench_adjoint(rank):
             f_ms, b_ms, _, g, c = ro.timed(U, cs, steps, gUT)
             fw.append(f_ms)
             bw.append(b_ms)
-        res[name] = dict(fwd_ms=min(fw), bwd_ms=min(bw), loss=float(loss), g=g[..., : ro.nk].to(torch.complex128),
+        res[name] = dict(fwd_ms=min(fw), bwd_ms=min(bw), loss=float(loss.detach()), g=g[..., : ro.nk].to(torch.complex128),
                          cs=float(c[0]), ro=ro, U=U)
     r32, r64 = res["f32"], res["f64"]
     # central difference in Cs on the FP64 path
@@ -473,6 +508,8 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
+    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble"],
+                    help="run one extra block alone and print it (profiling; not a bench line)")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference", "at least 3 warm-up steps"
 
@@ -506,9 +543,16 @@ def main():
     n = args.n
     npts = float(n) ** 3
     step = RK3_method.solveForNextTimestep
+    if args.only:
+        peak, _ = measured_peak()
+        fn = {"n512": lambda: bench_512(peak, rank), "adjoint": lambda: bench_adjoint(rank),
+              "ensemble": lambda: bench_ensemble(rank)}[args.only]
+        print(json.dumps({"only": args.only, "result": fn()}))
+        return
 
     # ---------------- device-resident FP32 run (value) ----------------
     d = make_domain(n, "float32", seed=rank)
+    tuned = tune_domain(d)
     for _ in range(args.warmup):
         step(d)
     _stepper.LAUNCHES[0] = 0
@@ -559,7 +603,7 @@ def main():
            "config": {"workload": workload_name(n), "n": n, "scheme": "RK3 (reference arithmetic)",
                       "les": "Smagorinsky", "precision": "fp32 fields/FFTs, fp64 twiddles",
                       "l2": "inputs larger than L2 (state 3x3x%.0f MB + workspace 9 fields)" % (fbytes / 1e6),
-                      "parallelism": "replicas" if world > 1 else "single GPU"},
+                      "parallelism": "replicas" if world > 1 else "single GPU", "autotune": tuned},
            "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": io_bytes,
                    "d2h_bytes_per_step": io_bytes, "steps": ke,
                    "path": "domain.U_hat <- pinned host; RK3_method.solveForNextTimestep; pinned host <- U_hat"},
@@ -586,6 +630,7 @@ def main():
             step(d32)
         a, bref = d32.U_hat.to(torch.complex128), d64.U_hat
         err = float(torch.linalg.vector_norm(a - bref) / torch.linalg.vector_norm(bref))
+        ek, klive, ekall = spectrum_error(a, bref, n)
         v64 = npts * kc / s64 / 1e6
         del d32, d64, a, bref
         torch.cuda.empty_cache()
@@ -596,6 +641,8 @@ def main():
                        "speedup_vs_fused_fp64": round(value / world / v64, 2),
                        "speedup_vs_torch_fp64": round(value / world / vtp, 2),
                        "rel_l2_fp32_vs_fp64": err, "steps_compared": kc + 2,
+                       "ek_err_fp32_vs_fp64": {"max_rel_shells_above_1e-8_of_peak": ek, "up_to_shell": klive,
+                                               "max_rel_all_shells": ekall},
                        "note": "FP32 fused vs FP64 fused (same kernels, float64) on the same seeded field"}
     if not args.no_compare and world == 1:
         out["n512"] = bench_512(peak, rank)

@@ -79,6 +79,20 @@ typedef struct sles_layout {
 int sles_plan_create(const sles_plan_desc* desc, sles_plan** out);
 int sles_plan_destroy(sles_plan* plan);
 int sles_plan_layout(const sles_plan* plan, sles_layout* out);
+/*
+ * Kernel variants (no counterpart in the reference): some passes are compiled
+ * in several tile geometries; which one runs is a plan setting, chosen by
+ * default per grid size and precision or by the autotuner (sles/autotune.py),
+ * which times each.  Every variant computes the same arithmetic (results agree
+ * to the last bit or, where the compiler contracts a*b+c differently, to round-off).
+ *   SLES_PASS_X: the x pass (stage update); variants 0..count-1
+ * sles_plan_variant_count returns 0 for a pass without variants;
+ * sles_plan_get_variant returns -1 for an invalid pass.
+ */
+enum { SLES_PASS_X = 0 };
+int sles_plan_variant_count(const sles_plan* plan, int pass);
+int sles_plan_get_variant(const sles_plan* plan, int pass);
+int sles_plan_set_variant(sles_plan* plan, int pass, int variant);
 /* Bytes of device workspace the plan needs for intermediate fields. */
 size_t sles_plan_workspace_bytes(const sles_plan* plan);
 /* Attach caller-owned device workspace (>= sles_plan_workspace_bytes). */

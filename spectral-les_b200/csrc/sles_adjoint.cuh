@@ -85,9 +85,9 @@ __device__ __forceinline__ void adj_project(typename CT<Tp>::C (&s)[3], const in
 // AX pass.  Work item = (ky slice, chunk of W kz columns); lines along x.
 // ---------------------------------------------------------------------------
 template <typename Tp, int N, class F>
-__global__ void __launch_bounds__(XGeo<Tp, N, F, 3>::THREADS, XGeo<Tp, N, F, 3>::MINB)
+__global__ void __launch_bounds__(XGeo<Tp, N, F, 3, 0>::THREADS, XGeo<Tp, N, F, 3, 0>::MINB)
 k_adj_xpass(const __grid_constant__ AXArgs<Tp> A) {
-  using K = XGeo<Tp, N, F, 3>;
+  using K = XGeo<Tp, N, F, 3, 0>;
   using C = typename CT<Tp>::C;
   constexpr int T = K::T, V = K::V, W = K::W;
   extern __shared__ __align__(1024) unsigned char smem_raw[];

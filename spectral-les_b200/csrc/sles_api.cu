@@ -80,7 +80,25 @@ int sles_plan_create(const sles_plan_desc* d, sles_plan** out) {
   I.ws_fields = eng->ws_fields_needed(I);
   I.flags = nullptr;
   I.scal = nullptr;
+  I.xvar = eng->default_xvar();
   *out = p;
+  return SLES_OK;
+}
+
+int sles_plan_variant_count(const sles_plan* p, int pass) {
+  if (!p) return 0;
+  return pass == SLES_PASS_X ? sles::X_VARIANTS : 0;
+}
+
+int sles_plan_get_variant(const sles_plan* p, int pass) {
+  if (!p || pass != SLES_PASS_X) return -1;
+  return p->info.xvar;
+}
+
+int sles_plan_set_variant(sles_plan* p, int pass, int variant) {
+  if (!p || pass != SLES_PASS_X) return SLES_ERR_INVALID_ARG;
+  if (variant < 0 || variant >= sles::X_VARIANTS) return SLES_ERR_INVALID_ARG;
+  p->info.xvar = variant;
   return SLES_OK;
 }
 

@@ -96,6 +96,24 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                : "memory");
 }
 
+// Per-thread asynchronous copy of one complex element (8 or 16 bytes) from
+// global to shared memory; pred = false zero-fills without reading.  A thread
+// waits for its own groups only (cp.async.wait_group), so a buffer that each
+// thread fills and later reads at the same positions needs no block barrier.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_el(void* dst, const void* src, bool pred) {
+  static_assert(BYTES == 8 || BYTES == 16, "8- or 16-byte elements");
+  if (BYTES == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(pred ? 8 : 0)
+                 : "memory");
+  else
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(pred ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(NPEND) : "memory"); }
+
 // exp(sign * 2 pi i e / m) computed in float64 and rounded once to Tp
 template <typename Tp>
 __device__ __forceinline__ typename CT<Tp>::C twiddle(long long e, long long m, int sign) {

@@ -26,6 +26,7 @@ struct PlanInfo {
   int ws_fields;         // half-complex field slots in the workspace
   unsigned* flags;       // device error word inside the workspace
   double* scal;          // device scalar scratch inside the workspace (64 doubles)
+  int xvar;              // x-pass variant (XGeo), set by default or by the autotuner
 };
 
 // workspace header: error word + scalar scratch, then the diagnostics area,
@@ -40,6 +41,7 @@ inline size_t slots_offset(int dim, int n) { return ((WS_HEADER + diag_area_byte
 struct Engine {
   virtual ~Engine() {}
   virtual int ws_fields_needed(const PlanInfo& p) const = 0;
+  virtual int default_xvar() const = 0;
   virtual int fft_r2c(PlanInfo& p, const void* in, void* out, int nf, cudaStream_t st) = 0;
   virtual int fft_c2r(PlanInfo& p, const void* in, void* out, int nf, cudaStream_t st) = 0;
   virtual int velocity_curl(PlanInfo& p, const void* uh, void* u, void* curl, cudaStream_t st) = 0;
@@ -238,14 +240,24 @@ struct EngineImpl final : Engine {
   // x pass: exchange padding divisor SLES_X_PADD (0: the plan's first radix)
   using FX = typename WithPad<typename PlanLo<Tp, N>::F, SLES_X_PADD>::F;
   using FY = typename PlanLo<Tp, N>::F;
-  static constexpr int W = XGeo<Tp, N, FX, DIM>::W;
   static constexpr int TZ = PlanFor<Tp, N / 2>::F::T;
   static constexpr int LPI = cmax(1, 16 / TZ);
 
   static C* slot(const PlanInfo& p, int i) {
     return reinterpret_cast<C*>(reinterpret_cast<char*>(p.ws) + slots_offset(DIM, N)) + (long long)i * p.hc_elems;
   }
-  static int nchunks(const PlanInfo& p) { return (p.nk + W - 1) / W; }
+  template <int XV>
+  static int xchunks(const PlanInfo& p) {  // x-pass column chunks of variant XV
+    constexpr int WX = XGeo<Tp, N, FX, DIM, XV>::W;
+    return (p.nk + WX - 1) / WX;
+  }
+  // x-pass variant used until a caller (the autotuner) sets another: the
+  // 32-byte-row ring for float32 3D grids of 64^3 and up, else direct loads
+  int default_xvar() const override { return (sizeof(Tp) == 4 && DIM == 3 && N >= 64) ? 2 : 0; }
+  static int ychunks(const PlanInfo& p) {                                 // y-pass column chunks
+    constexpr int WY = TGeo<Tp, N, FY>::W;
+    return (p.nk + WY - 1) / WY;
+  }
 
   int ws_fields_needed(const PlanInfo& p) const override {
     const bool les = p.d.les_model != SLES_LES_NONE;
@@ -290,7 +302,6 @@ struct EngineImpl final : Engine {
     a.fs = p.hc_elems;
     a.nkp = p.nkp;
     a.nk = p.nk;
-    a.nchunks = nchunks(p);
     a.nu = (Tp)p.d.nu;
     a.forcing = (Tp)p.d.forcing;
     a.kmax = 2.0 / 3.0 * (double)(N / 2 + 1);  // initialize_domain.py:79
@@ -311,7 +322,16 @@ struct EngineImpl final : Engine {
 
   template <int LES, int PAR2D>
   int xpass(const PlanInfo& p, XArgs<Tp> a, cudaStream_t st) {
-    using K = XGeo<Tp, N, FX, DIM>;
+    switch (p.xvar) {
+      case 1: return xpass_v<LES, PAR2D, 1>(p, a, st);
+      case 2: return xpass_v<LES, PAR2D, 2>(p, a, st);
+      default: return xpass_v<LES, PAR2D, 0>(p, a, st);
+    }
+  }
+  template <int LES, int PAR2D, int XV>
+  int xpass_v(const PlanInfo& p, XArgs<Tp> a, cudaStream_t st) {
+    using K = XGeo<Tp, N, FX, DIM, XV>;
+    a.nchunks = xchunks<XV>(p);
     // state tiles the stage reads (ucur for viscous/forcing/update; u0 when
     // distinct from ucur; u1 = RK4 accumulator or ETD2's previous F1)
     a.need_uc = a.need_u0 = a.need_u1 = 0;
@@ -322,8 +342,10 @@ struct EngineImpl final : Engine {
       a.need_u1 = (a.kind == KX_RK4 || a.kind == KX_ETD2P || a.kind == KX_ETD2C) ? 1 : 0;
     }
     a.err = p.flags;
-    const long long items = (long long)(DIM == 3 ? N : 1) * nchunks(p);
-    return launch_persistent(k_xpass<Tp, N, FX, DIM, LES, PAR2D>, items, K::THREADS, K::SMEM, st, a);
+    const long long items = (long long)(DIM == 3 ? N : 1) * a.nchunks;
+    if (a.kind == KX_ETD2P || a.kind == KX_ETD2C)
+      return launch_persistent(k_xpass<Tp, N, FX, DIM, LES, PAR2D, 1, XV>, items, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_xpass<Tp, N, FX, DIM, LES, PAR2D, 0, XV>, items, K::THREADS, K::SMEM, st, a);
   }
   int xpass_rt(const PlanInfo& p, const XArgs<Tp>& a, int les, int par2d, cudaStream_t st) {
     if (!les) return xpass<0, 0>(p, a, st);
@@ -344,8 +366,8 @@ struct EngineImpl final : Engine {
     a.fs = p.hc_elems;
     a.nkp = p.nkp;
     a.nk = p.nk;
-    a.nchunks = nchunks(p);
-    const long long items = (long long)N * nchunks(p);
+    a.nchunks = ychunks(p);
+    const long long items = (long long)N * ychunks(p);
     if (inv) return launch_persistent(k_ypass<Tp, N, FY, LES, 1>, items, K::THREADS, K::SMEM, st, a);
     return launch_persistent(k_ypass<Tp, N, FY, LES, 0>, items, K::THREADS, K::SMEM, st, a);
   }
@@ -543,15 +565,15 @@ struct EngineImpl final : Engine {
     a.fs = pa.hc_elems;
     a.nkp = pa.nkp;
     a.nk = pa.nk;
-    a.nchunks = nchunks(pa);
+    a.nchunks = xchunks<0>(pa);
     a.nu = (Tp)pa.d.nu;
     a.forcing = (Tp)pa.d.forcing;
     a.kmax = 2.0 / 3.0 * (double)(N / 2 + 1);  // initialize_domain.py:79
     return a;
   }
   int axpass(const PlanInfo& pa, const AXArgs<Tp>& a, cudaStream_t st) {
-    using K = XGeo<Tp, N, FX, 3>;
-    const long long items = (long long)N * nchunks(pa);
+    using K = XGeo<Tp, N, FX, 3, 0>;
+    const long long items = (long long)N * xchunks<0>(pa);
     return launch_persistent(k_adj_xpass<Tp, N, FX>, items, K::THREADS, K::SMEM, st, a);
   }
   template <int MODEL>
@@ -586,8 +608,8 @@ struct EngineImpl final : Engine {
     a.fs = pa.hc_elems;
     a.nkp = pa.nkp;
     a.nk = pa.nk;
-    a.nchunks = nchunks(pa);
-    const long long items = (long long)N * nchunks(pa);
+    a.nchunks = ychunks(pa);
+    const long long items = (long long)N * ychunks(pa);
     if (inv) return launch_persistent(k_ypass<Tp, N, FY, 1, 1, 1>, items, K::THREADS, K::SMEM, st, a);
     return launch_persistent(k_ypass<Tp, N, FY, 1, 0, 1>, items, K::THREADS, K::SMEM, st, a);
   }

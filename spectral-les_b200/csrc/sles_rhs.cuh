@@ -96,7 +96,9 @@ __device__ __forceinline__ void project(const XArgs<Tp>& A, typename CT<Tp>::C (
 // Stage update of one component at one position.  R: projected term of
 // component c; uc/u0/u1: state values at this position (u1: RK4 accumulator
 // or ETD2's previous F1).  Writes uout/u1/aux and returns the new state.
-template <typename Tp>
+// ETD = 0 drops the exponential schemes (their float64 weights) from the
+// kernel, which keeps the Runge-Kutta kernels' register count down.
+template <typename Tp, int ETD>
 __device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& A, int c, typename CT<Tp>::C R,
                                                               typename CT<Tp>::C uc, typename CT<Tp>::C u0,
                                                               typename CT<Tp>::C u1, int k2, long long off) {
@@ -109,7 +111,7 @@ __device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& 
   if (A.forcing > (Tp)0 && k2 != 0) R = cadd(R, cscale(uc, A.forcing));  // RK4_method.py:58-64
   if (A.record_f1) A.aux[o] = (A.record_f1 == 2) ? csub(R, A.aux[o]) : R;  // RK4_method.py:65-66
   C un;
-  if (A.kind == KX_ETD2P || A.kind == KX_ETD2C) {
+  if (ETD && (A.kind == KX_ETD2P || A.kind == KX_ETD2C)) {
     // parity: src/ETD2_method.py:16-29; corrected: Cox & Matthews (2002) eq. 22
     const double z = A.dt_d * A.nu_d * (double)k2;
     const double E = exp(-A.dt_d * A.nu_d * (double)k2);
@@ -198,21 +200,34 @@ struct TGeo {
   static constexpr int MINB = (sizeof(Tp) == 4) ? (THREADS >= 512 ? 1 : (THREADS >= 256 ? SLES_T_MINB256 : 4)) : 1;
 };
 
-// x-pass geometry: direct coalesced loads, the projected components kept in
-// a shared stash [D][N][W] between the forward and the per-component phase
-template <typename Tp, int N, class F, int DIM>
+// x-pass geometry: the projected components kept in a shared stash
+// [D][N][W] between the forward and the per-component phase.  Variants XV
+// (picked at run time, by default or by the autotuner):
+//   0: W = 64-byte tile rows, direct loads, 16 warps per SM (FP32)
+//   1: W = 64-byte rows, the item's tiles [N][W] prefetched one ahead into a
+//      ring of 2 buffers with per-thread cp.async, 8 warps per SM
+//   2: W = 32-byte rows, the same ring, 12 warps per SM
+// A ring that does not fit the variant's shared-memory budget falls back to
+// direct loads (NB = 0).
+constexpr int X_VARIANTS = 3;
+template <typename Tp, int N, class F, int DIM, int XV>
 struct XGeo {
   using C = typename CT<Tp>::C;
-  static constexpr int W = (sizeof(Tp) == 4) ? 8 : 4;
+  static constexpr bool F32 = sizeof(Tp) == 4;
+  static constexpr int W = (XV == 2) ? (F32 ? 4 : 2) : (F32 ? 8 : 4);
   static constexpr int T = F::T, V = F::V;
   static constexpr int THREADS = W * T;
   static constexpr int TE = N * W;
   static constexpr int SCR = F::XLEN * W;
-  static constexpr size_t SMEM = ((size_t)DIM * TE + SCR + N) * sizeof(C);  // + linear twiddle table
-#ifndef SLES_X_MINB256
-#define SLES_X_MINB256 2
-#endif
-  static constexpr int MINB = (sizeof(Tp) == 4) ? (THREADS >= 512 ? 1 : (THREADS >= 256 ? SLES_X_MINB256 : 4)) : 1;
+  static constexpr int WARPS = (THREADS + 31) / 32;
+  static constexpr int TARGET = F32 ? (XV == 0 ? 16 : (XV == 1 ? 8 : 12)) : (XV == 2 ? 8 : WARPS);
+  static constexpr int MINB0 = TARGET / WARPS;
+  static constexpr int MINB = MINB0 < 1 ? 1 : (MINB0 > 16 ? 16 : MINB0);
+  static constexpr size_t BASE = ((size_t)DIM * TE + SCR + N) * sizeof(C);  // + linear twiddle table
+  // shared memory per block that keeps MINB blocks resident (228 KB per SM, 1 KB reserved per block)
+  static constexpr size_t BUDGET = (228 / MINB - 1) * 1024;
+  static constexpr int NB = (XV == 0) ? 0 : ((BASE + 2 * (size_t)TE * sizeof(C) <= BUDGET) ? 2 : 0);
+  static constexpr size_t SMEM = BASE + (size_t)NB * TE * sizeof(C);
 };
 
 // slot of tile `i` in a pass's per-item load sequence
@@ -235,16 +250,17 @@ __device__ __forceinline__ int seq_slot(int i) {
 // X pass.  Work item = (ky slice [3D], column chunk of W last-axis wavenumbers);
 // lines along x.  PAR2D selects the reference's 2D stress (1) or the corrected one.
 // ---------------------------------------------------------------------------
-template <typename Tp, int N, class F, int DIM, int LES, int PAR2D>
-__global__ void __launch_bounds__(XGeo<Tp, N, F, DIM>::THREADS, XGeo<Tp, N, F, DIM>::MINB)
+template <typename Tp, int N, class F, int DIM, int LES, int PAR2D, int ETD, int XV>
+__global__ void __launch_bounds__(XGeo<Tp, N, F, DIM, XV>::THREADS, XGeo<Tp, N, F, DIM, XV>::MINB)
 k_xpass(const __grid_constant__ XArgs<Tp> A) {
-  using K = XGeo<Tp, N, F, DIM>;
+  using K = XGeo<Tp, N, F, DIM, XV>;
   using C = typename CT<Tp>::C;
-  constexpr int T = K::T, V = K::V, D = DIM, W = K::W;
+  constexpr int T = K::T, V = K::V, D = DIM, W = K::W, NB = K::NB;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   C* rst = reinterpret_cast<C*>(smem_raw);  // [D][N][W] projected components
   C* sm0 = rst + D * K::TE;                 // exchange scratch
   C* twt = sm0 + K::SCR;                    // twiddle table exp(-2 pi i e/N)
+  C* ring = twt + N;                        // NB tile buffers [N][W]
   const int tid = threadIdx.x;
   const int l = tid % W, j = tid / W;
   F::fill_table_lin(twt);
@@ -258,16 +274,60 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
   C* ws = A.ws;
   auto kx_at = [&](int m) { return kc2c(j + T * m, N); };
   auto rpos = [&](int c, int m) { return c * K::TE + (j + T * m) * W + l; };
+  // the item's tile sequence: forward tiles (slots), then per component the
+  // state tiles the stage reads (ucur, u0, u1); inverse-only items: uinv
+  constexpr int NTF = LES ? (DIM == 3 ? 6 : (PAR2D ? 4 : 5)) : D;
+  const int nst = A.need_uc + A.need_u0 + A.need_u1;
+  const int TPI = A.fwd ? NTF + D * nst : D;
+  auto tile_src = [&](int k) -> const C* {
+    if (!A.fwd) return A.uinv + k * fs;
+    if (k < NTF) return ws + (LES && DIM == 3 ? seq_slot<4>(k) : k) * fs;
+    k -= NTF;
+    const int c = k / nst, r = k % nst;
+    int q = 0;
+    if (A.need_uc) { if (r == q) return A.ucur + c * fs; ++q; }
+    if (A.need_u0) { if (r == q) return A.u0 + c * fs; ++q; }
+    return A.u1 + c * fs;
+  };
+  long long tq = 0;  // next tile to consume
+  auto issue = [&](long long t) {  // prefetch tile t of this block's sequence (every thread its own positions)
+    if constexpr (NB > 0) {
+      const long long it2 = blockIdx.x + (t / TPI) * (long long)gridDim.x;
+      if (it2 < items) {
+        const int col2 = (int)(it2 % A.nchunks) * W + l;
+        const bool ok2 = col2 < A.nk;
+        const C* src = tile_src((int)(t % TPI)) + (it2 / A.nchunks) * A.nkp + (ok2 ? col2 : 0);
+        C* dst = ring + (int)(t % NB) * K::TE + j * W + l;
+#pragma unroll
+        for (int m = 0; m < V; ++m) cp_async_el<sizeof(C)>(dst + T * m * W, src + (j + T * m) * ps, ok2);
+      }
+      cp_async_commit();
+    }
+  };
+  if constexpr (NB > 0) {
+    for (int t = 0; t < NB - 1; ++t) issue(t);
+  }
   for (long long it = blockIdx.x; it < items; it += gridDim.x) {  // persistent over work items
     const int chunk = (int)(it % A.nchunks);
     const int sl = (int)(it / A.nchunks);  // ky slice (3D); 0 in 2D
     const int col = chunk * W + l;
     const bool ok = col < A.nk;
     const long long base = (long long)sl * A.nkp + col;
-    auto ld = [&](C (&v)[V], const C* src, int slot) {
+    // next tile of the sequence (its source is implied by the sequence position)
+    auto take = [&](C (&v)[V], const C* src, int slot) {
+      if constexpr (NB > 0) {
+        issue(tq + NB - 1);
+        cp_async_wait<NB - 1>();
+        const C* tl = ring + (int)(tq % NB) * K::TE + j * W + l;
 #pragma unroll
-      for (int m = 0; m < V; ++m) v[m] = ok ? src[slot * fs + base + (j + T * m) * ps] : cmk<C>(0, 0);
+        for (int m = 0; m < V; ++m) v[m] = tl[T * m * W];
+        ++tq;
+      } else {
+#pragma unroll
+        for (int m = 0; m < V; ++m) v[m] = ok ? src[slot * fs + base + (j + T * m) * ps] : cmk<C>(0, 0);
+      }
     };
+    auto ld = take;
     auto st = [&](int slot, const C (&v)[V]) {
       if (ok) {
 #pragma unroll
@@ -360,16 +420,29 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
 #pragma unroll 1
     for (int c = 0; c < D; ++c) {
       C v[V];
+      C ucv[NB > 0 ? V : 1], u0v[NB > 0 ? V : 1], u1v[NB > 0 ? V : 1];
+      if constexpr (NB > 0) {
+        if (A.need_uc) take(ucv, A.ucur, c);
+        if (A.need_u0) take(u0v, A.u0, c);
+        if (A.need_u1) take(u1v, A.u1, c);
+      }
       if (ok) {
 #pragma unroll
         for (int m = 0; m < V; ++m) {
           const long long off = base + (j + T * m) * ps;
           const int kx = kx_at(m);
           const int k2 = kx * kx + kyv * kyv + col * col;
-          const C ucm = A.need_uc ? A.ucur[c * fs + off] : cmk<C>(0, 0);
-          const C u0m = A.need_u0 ? A.u0[c * fs + off] : ucm;
-          const C u1m = A.need_u1 ? A.u1[c * fs + off] : cmk<C>(0, 0);
-          v[m] = update_component<Tp>(A, c, rst[rpos(c, m)], ucm, u0m, u1m, k2, off);
+          C ucm, u0m, u1m;
+          if constexpr (NB > 0) {
+            ucm = A.need_uc ? ucv[m] : cmk<C>(0, 0);
+            u0m = A.need_u0 ? u0v[m] : ucm;
+            u1m = A.need_u1 ? u1v[m] : cmk<C>(0, 0);
+          } else {
+            ucm = A.need_uc ? A.ucur[c * fs + off] : cmk<C>(0, 0);
+            u0m = A.need_u0 ? A.u0[c * fs + off] : ucm;
+            u1m = A.need_u1 ? A.u1[c * fs + off] : cmk<C>(0, 0);
+          }
+          v[m] = update_component<Tp, ETD>(A, c, rst[rpos(c, m)], ucm, u0m, u1m, k2, off);
         }
       } else {
 #pragma unroll

@@ -26,7 +26,9 @@ EXPORTED = [
     "sles_velocity_curl", "sles_velocity_gradient", "sles_rhs", "sles_stage", "sles_diag",
     "sles_status_string", "sles_version", "sles_profile_rhs", "sles_rhs_static_workspace",
     "sles_adjoint_workspace_bytes", "sles_adjoint_seed", "sles_adjoint_prime", "sles_adjoint_stage",
+    "sles_plan_variant_count", "sles_plan_get_variant", "sles_plan_set_variant",
 ]
+PASS_X = 0
 
 
 class PlanDesc(ctypes.Structure):
@@ -78,6 +80,9 @@ def load_library(path: str = LIB_PATH):
         "sles_profile_rhs": (i, [vp, vp, vp, i, vp, vp]),
         "sles_rhs_static_workspace": (i, [vp, vp, vp, vp, vp, vp, vp]),
         "sles_version": (i, []),
+        "sles_plan_variant_count": (i, [vp, i]),
+        "sles_plan_get_variant": (i, [vp, i]),
+        "sles_plan_set_variant": (i, [vp, i, i]),
         "sles_adjoint_workspace_bytes": (ctypes.c_size_t, [vp]),
         "sles_adjoint_seed": (i, [vp, vp, d, vp, vp, vp, vp]),
         "sles_adjoint_prime": (i, [vp, vp, vp, vp, vp]),
@@ -129,6 +134,15 @@ class Plan:
         self._ws_ptr = self.workspace.data_ptr() + off
         check(L.sles_plan_set_workspace(h, ctypes.c_void_p(self._ws_ptr), ctypes.c_size_t(nbytes)),
               "sles_plan_set_workspace")
+
+    def variant_count(self, pass_=PASS_X):
+        return int(self.L.sles_plan_variant_count(self.h, int(pass_)))
+
+    def get_variant(self, pass_=PASS_X):
+        return int(self.L.sles_plan_get_variant(self.h, int(pass_)))
+
+    def set_variant(self, variant, pass_=PASS_X):
+        check(self.L.sles_plan_set_variant(self.h, int(pass_), int(variant)), "sles_plan_set_variant")
 
     def set_params(self, nu, cs, forcing):
         check(self.L.sles_plan_set_params(self.h, float(nu), float(cs), float(forcing)), "sles_plan_set_params")

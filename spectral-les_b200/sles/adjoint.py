@@ -24,6 +24,7 @@ import math
 import torch
 
 from . import _native as nat
+from . import autotune
 
 __all__ = ["RK4Rollout", "shell_spectrum", "log_spectrum_misfit"]
 
@@ -50,6 +51,7 @@ class RK4Rollout:
         self.cdtype = torch.complex64 if dtype == torch.float32 else torch.complex128
         self.device = torch.device(device)
         self.plan = nat.Plan(3, self.n, dtype, model, nat.SCHEME_RK4, parity, nu, Cs, forcing, self.device)
+        autotune.apply_cached(self.plan, "RK4")
         self.nk, self.nkp = self.plan.nk, self.plan.nkp
         self._ws_owner, self._ws = self.plan.adjoint_workspace()
         self._store = []   # stage states of the segment being reversed (reused across calls)

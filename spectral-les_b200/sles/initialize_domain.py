@@ -27,6 +27,7 @@ import numpy as np
 import torch
 
 from . import _native as nat
+from . import autotune
 
 __all__ = ["InitializeDomain"]
 
@@ -147,6 +148,7 @@ class InitializeDomain:
         scheme = {"RK4": nat.SCHEME_RK4, "RK3": nat.SCHEME_RK3, "ETD2": nat.SCHEME_ETD2}[method]
         self._plan = nat.Plan(self.dim, self.N, self._rdtype, les, scheme, self.parity_mode, nu, Cs,
                               forcing, self.device)
+        autotune.apply_cached(self._plan, method)  # kernel variants recorded by sles.autotune.tune
         self._nk, self._nkp = self._plan.nk, self._plan.nkp
         self._hc_shape = self.shape[:-1] + (self._nk,)
         self._hc_pshape = self.shape[:-1] + (self._nkp,)

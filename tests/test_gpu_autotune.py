@@ -1,0 +1,80 @@
+"""Kernel variants and the autotuner: every x-pass variant gives the same
+states (bit-identical in the float32 cases here; float64 up to the compiler's
+floating-point contraction, 1e-14 relative); tune() picks one, records it and
+new domains pick it up."""
+import json
+
+import pytest
+import torch
+
+from sles import autotune, RK3_method, RK4_method, ETD2_method
+from sles import _native as nat
+from sles.initial import initial_velocity, initial_vorticity
+from sles.initialize_domain import InitializeDomain
+from sles.synthetic import gaussian_vorticity_2d, random_spectrum_velocity
+
+pytestmark = pytest.mark.gpu
+
+STEP = {"RK3": RK3_method.solveForNextTimestep, "RK4": RK4_method.solveForNextTimestep,
+        "ETD2": ETD2_method.solveForNextTimestep}
+CASES = [  # (dim, n, dtype, les, method, parity)
+    (3, 64, "float32", "Smagorinsky", "RK3", True),
+    (3, 96, "float32", "vreman", "RK4", True),
+    (3, 128, "float32", "Smagorinsky", "ETD2", False),
+    (3, 48, "float64", "Smagorinsky", "RK4", True),
+    (3, 64, "float32", None, "RK4", True),
+    (2, 256, "float32", None, "RK4", True),
+]
+
+
+def _dom(dim, n, dtype, les, method, parity):
+    d = InitializeDomain(nu=1e-3, dimension=dim, time_stepSize=1e-3, No_of_gridpoint=(4 if les else 1) * n,
+                         method=method, LES_ON=1 if les else 0, LES_model=les, Cs=0.17, dtype=dtype,
+                         parity_mode=parity)
+    if dim == 3:
+        initial_velocity(d, *random_spectrum_velocity(n, 4.0, 1.0, seed=2))
+    else:
+        initial_vorticity(d, gaussian_vorticity_2d(n, seed=2))
+    d.U_hat1[...] = d.U_hat
+    return d
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "%dd%d_%s_%s_%s" % (c[0], c[1], c[2], c[3], c[4]))
+def test_variants_are_bit_identical(case):
+    ref = None
+    for v in range(3):
+        d = _dom(*case)
+        assert d._plan.variant_count(nat.PASS_X) == 3
+        d._plan.set_variant(v, nat.PASS_X)
+        for _ in range(3):
+            STEP[case[4]](d)
+        u = d.U_hat.clone()
+        if ref is None:
+            ref = u
+        elif case[2] == "float32":
+            assert torch.equal(u, ref), "x-pass variant %d differs" % v
+        else:
+            rel = float(torch.linalg.vector_norm(u - ref) / torch.linalg.vector_norm(ref))
+            assert rel < 1e-14, "x-pass variant %d differs by %g" % (v, rel)
+
+
+def test_tune_records_and_reapplies(tmp_path, monkeypatch):
+    monkeypatch.setenv("SLES_TUNE_CACHE", str(tmp_path / "tune.json"))
+    d = _dom(3, 64, "float32", "Smagorinsky", "RK3", True)
+    before = d.U_hat.clone()
+    times = autotune.tune(d, steps=2, repeats=2)
+    assert set(times) == {0, 1, 2} and all(t > 0 for t in times.values())
+    win = min(times, key=times.get)
+    assert d._plan.get_variant(nat.PASS_X) == win
+    assert torch.equal(d.U_hat, before)  # tuning does not advance the domain
+    table = json.loads((tmp_path / "tune.json").read_text())
+    key = autotune.plan_key(d._plan, "RK3")
+    assert table[key]["variants"][str(nat.PASS_X)] == win
+    d2 = _dom(3, 64, "float32", "Smagorinsky", "RK3", True)
+    assert d2._plan.get_variant(nat.PASS_X) == win
+    # stepping after tuning matches an untuned domain
+    d3 = _dom(3, 64, "float32", "Smagorinsky", "RK3", True)
+    for _ in range(2):
+        RK3_method.solveForNextTimestep(d)
+        RK3_method.solveForNextTimestep(d3)
+    assert torch.equal(d.U_hat, d3.U_hat)
