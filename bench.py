@@ -33,6 +33,7 @@ NU, CS, DT, K0, U0 = 1e-4, 0.17, 1e-3, 4.0, 1.0
 # algorithmic HBM bytes per grid point per RHS evaluation (3D LES, FP32): 21 transforms
 # x 16 B (two out-of-cache passes, read+write) + 48 B integrator state
 STEP_BYTES_PER_PT_RHS = {"f32": 384.0, "f64": 768.0}
+TUNE = True  # run the autotuner on each timed domain (outside the timed regions)
 
 
 def workload_name(n):
@@ -172,7 +173,7 @@ def tune_domain(d):
     from sles import autotune
     if not os.environ.get("SLES_TUNE_CACHE"):
         os.environ["SLES_TUNE_CACHE"] = os.path.join(tempfile.gettempdir(), "sles_bench_tune_%d.json" % os.getpid())
-    times = autotune.tune(d)
+    times = autotune.tune(d) if TUNE else {}
     return {"x_pass_variant": d._plan.get_variant(0), "ms_per_step_by_variant": {str(k): round(v, 4)
                                                                                   for k, v in times.items()}}
 
@@ -508,10 +509,14 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner (use the default or cached kernel variants)")
     ap.add_argument("--only", choices=["n512", "adjoint", "ensemble"],
                     help="run one extra block alone and print it (profiling; not a bench line)")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference", "at least 3 warm-up steps"
+    global TUNE
+    TUNE = not args.no_tune
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -347,6 +347,7 @@ k_adj_zpass(const AZArgs<Tp> A) {
   using F = typename K::F;
   using C = typename CT<Tp>::C;
   constexpr int T = K::T, V = K::V, NKP = K::NKP, SFS = LPI * K::RS;
+  constexpr int WS = (T <= 32 && 32 % T == 0) ? 1 : 0;  // a line's threads share one warp
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
   C* twN = reinterpret_cast<C*>(smem_raw + K::OFF_TW);
@@ -402,8 +403,8 @@ k_adj_zpass(const AZArgs<Tp> A) {
         else x = cmuli_s(sb[s2 * LPI * NKP + k], (Tp)k);
         return x;
       });
-      fft.template run<+1>(v, j, sm, 1);
-      __syncthreads();
+      fft.template run<+1, WS>(v, j, sm, 1);
+      F::template lsync<WS>();
       const Tp sc = r == 0 ? A.scale : (Tp)1;
 #pragma unroll
       for (int m = 0; m < V; ++m) sm[j + T * m] = cscale(v[m], sc);
@@ -425,8 +426,8 @@ k_adj_zpass(const AZArgs<Tp> A) {
       C v[V];
 #pragma unroll
       for (int m = 0; m < V; ++m) v[m] = sm[j + T * m];
-      fft.template run<-1>(v, j, sm, 1);
-      r2c_post<F>(v, j, sm, 1, twN, [&](int k, C x) { spec[k] = x; });
+      fft.template run<-1, WS>(v, j, sm, 1);
+      r2c_post<F, WS>(v, j, sm, 1, twN, [&](int k, C x) { spec[k] = x; });
     }
     __syncthreads();
     // ---- phase D: Z_c = ubar_c - i kz abar_3c, A1_c, A2_c with weights w/N^3

@@ -252,8 +252,14 @@ struct EngineImpl final : Engine {
     return (p.nk + WX - 1) / WX;
   }
   // x-pass variant used until a caller (the autotuner) sets another: the
-  // 32-byte-row ring for float32 3D grids of 64^3 and up, else direct loads
-  int default_xvar() const override { return (sizeof(Tp) == 4 && DIM == 3 && N >= 64) ? 2 : 0; }
+  // fastest in a timing sweep of every size on a B200 (RK3 Smagorinsky and
+  // RK4 without LES; see sles/autotune.py)
+  int default_xvar() const override {
+    if (sizeof(Tp) == 8) return (DIM == 2 && N >= 1024) ? 0 : (DIM == 2 ? 2 : 1);
+    if (DIM == 2) return 2;
+    if (N <= 64) return 1;
+    return (N == 128 || N == 256) ? 2 : 0;
+  }
   static int ychunks(const PlanInfo& p) {                                 // y-pass column chunks
     constexpr int WY = TGeo<Tp, N, FY>::W;
     return (p.nk + WY - 1) / WY;

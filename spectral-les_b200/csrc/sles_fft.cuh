@@ -256,18 +256,33 @@ struct LineFFT {
     }
   }
 
+  // Barrier among the threads that share a line's exchange scratch: the whole
+  // block (WS = 0, lines spread over warps) or only the line's own T
+  // consecutive lanes of one warp (WS = 1).
+  template <int WS>
+  __device__ __forceinline__ static void lsync() {
+    if constexpr (WS) {
+      static_assert(T <= 32 && 32 % T == 0, "a line's threads must lie in one warp");
+      const unsigned lane = threadIdx.x & 31u;
+      const unsigned m = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << (lane / T * T));
+      __syncwarp(m);
+    } else {
+      __syncthreads();
+    }
+  }
+
   // Transform with twiddles from `tab` (L entries, see fill_table); needs no init().
-  template <int DIR, bool LIN = false>
+  template <int DIR, bool LIN = false, int WS = 0>
   __device__ __forceinline__ void run_tab(C (&v)[V], int j, C* sm, int ws, const C* tab) {
-    if constexpr (S >= 2) __syncthreads();
+    if constexpr (S >= 2) lsync<WS>();
     stage_tab<R0, DIR, S == 1, LIN>(v, tab, 1, j, sm, ws);
     if constexpr (S >= 2) {
-      exchange(v, j, sm, ws);
-      if constexpr (S >= 3) __syncthreads();
+      exchange<WS>(v, j, sm, ws);
+      if constexpr (S >= 3) lsync<WS>();
       stage_tab<R1, DIR, S == 2, LIN>(v, tab, R0, j, sm, ws);
     }
     if constexpr (S >= 3) {
-      exchange(v, j, sm, ws);
+      exchange<WS>(v, j, sm, ws);
       stage_tab<R2, DIR, true, LIN>(v, LIN ? tab : tab + TAB1, R0 * R1, j, sm, ws);
     }
   }
@@ -290,28 +305,30 @@ struct LineFFT {
     }
   }
 
+  template <int WS = 0>
   __device__ __forceinline__ void exchange(C (&v)[V], int j, C* sm, int ws) {
-    __syncthreads();
+    lsync<WS>();
 #pragma unroll
     for (int m = 0; m < V; ++m) v[m] = sm[pad(j + T * m) * ws];
   }
 
   // In-place transform of the cyclic registers.  sm: this line's exchange
-  // scratch (XLEN slots of stride ws).  All threads of the block must
-  // call this uniformly (it contains __syncthreads when S > 1).  Convention
-  // shared by every user of an exchange scratch: a barrier precedes each
-  // write phase, so back-to-back transforms on one scratch are safe.
-  template <int DIR>
+  // scratch (XLEN slots of stride ws).  With WS = 0 all threads of the block
+  // must call this uniformly (it contains __syncthreads when S > 1); with
+  // WS = 1 only the line's own lanes.  Convention shared by every user of an
+  // exchange scratch: a barrier precedes each write phase, so back-to-back
+  // transforms on one scratch are safe.
+  template <int DIR, int WS = 0>
   __device__ __forceinline__ void run(C (&v)[V], int j, C* sm, int ws) {
-    if constexpr (S >= 2) __syncthreads();
+    if constexpr (S >= 2) lsync<WS>();
     stage<R0, DIR, S == 1, false>(v, tw1, 1, j, sm, ws);
     if constexpr (S >= 2) {
-      exchange(v, j, sm, ws);
-      if constexpr (S >= 3) __syncthreads();
+      exchange<WS>(v, j, sm, ws);
+      if constexpr (S >= 3) lsync<WS>();
       stage<R1, DIR, S == 2, true>(v, tw1, R0, j, sm, ws);
     }
     if constexpr (S >= 3) {
-      exchange(v, j, sm, ws);
+      exchange<WS>(v, j, sm, ws);
       stage<R2, DIR, true, true>(v, tw2, R0 * R1, j, sm, ws);
     }
   }
@@ -374,16 +391,17 @@ __device__ __forceinline__ void c2r_pre(typename F::C (&v)[F::V], int j, const t
 
 // r2c post-processing.  v holds Z = FFT_L(z) with z[n] = x[2n] + i x[2n+1];
 // emits out(k, X_k) for k in [0, L] (bin L by thread j == 0).  Uses the line's
-// exchange scratch; all threads of the block must call it uniformly.
-template <class F, class Dst>
+// exchange scratch; all threads of the block (WS = 0) or the line's lanes
+// (WS = 1) must call it uniformly.
+template <class F, int WS = 0, class Dst>
 __device__ __forceinline__ void r2c_post(typename F::C (&v)[F::V], int j, typename F::C* sm, int ws,
                                          const typename F::C* twN, Dst out) {
   using C = typename F::C;
   using Tp = decltype(C::x);
-  __syncthreads();
+  F::template lsync<WS>();
 #pragma unroll
   for (int m = 0; m < F::V; ++m) sm[F::pad(j + F::T * m) * ws] = v[m];
-  __syncthreads();
+  F::template lsync<WS>();
 #pragma unroll
   for (int m = 0; m < F::V; ++m) {
     int k = j + F::T * m;

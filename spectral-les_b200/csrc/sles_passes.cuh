@@ -81,6 +81,7 @@ struct RealAxis {
   static constexpr int THREADS = LPB * T;
   static constexpr int LS = ((F::XLEN + 15) / 16) * 16 + 8;  // line stride of the scratch
   static constexpr size_t SMEM = ((size_t)LPB * LS + L) * sizeof(C);
+  static constexpr int WS = (T <= 32 && 32 % T == 0) ? 1 : 0;  // a line's threads share one warp
 };
 
 template <typename Tp, int NR, int LPB>
@@ -92,6 +93,7 @@ k_r2c_line(const Tp* __restrict__ src, typename CT<Tp>::C* __restrict__ dst, lon
   C* twN = reinterpret_cast<C*>(smem_raw);
   C* scr = twN + K::L;
   fill_twN<Tp, NR>(twN);
+  __syncthreads();  // twN is read by every line (its barriers may be line-level only)
   const int tid = threadIdx.x;
   const int j = tid % K::T, ln = tid / K::T;
   typename K::F fft;
@@ -105,8 +107,8 @@ k_r2c_line(const Tp* __restrict__ src, typename CT<Tp>::C* __restrict__ dst, lon
     C v[K::F::V];
 #pragma unroll
     for (int m = 0; m < K::F::V; ++m) v[m] = ok ? in[j + K::T * m] : cmk<C>(0, 0);
-    fft.template run<-1>(v, j, scr + ln * K::LS, 1);
-    r2c_post<typename K::F>(v, j, scr + ln * K::LS, 1, twN, [&](int k, C x) {
+    fft.template run<-1, K::WS>(v, j, scr + ln * K::LS, 1);
+    r2c_post<typename K::F, K::WS>(v, j, scr + ln * K::LS, 1, twN, [&](int k, C x) {
       if (ok) out[k] = x;
     });
   }
@@ -135,7 +137,7 @@ k_c2r_line(const typename CT<Tp>::C* __restrict__ src, Tp* __restrict__ dst, lon
     C* out = reinterpret_cast<C*>(dst + (ok ? line : 0) * NR);
     C v[K::F::V];
     c2r_pre<typename K::F>(v, j, twN, [&](int k) { return ok ? in[k] : cmk<C>(0, 0); });
-    fft.template run<+1>(v, j, scr + ln * K::LS, 1);
+    fft.template run<+1, K::WS>(v, j, scr + ln * K::LS, 1);
     if (ok) {
 #pragma unroll
       for (int m = 0; m < K::F::V; ++m) out[j + K::T * m] = cscale(v[m], scale);

@@ -792,6 +792,7 @@ k_zpass(const ZArgs<Tp> A) {
   using F = typename K::F;
   using C = typename CT<Tp>::C;
   constexpr int T = K::T, V = K::V, NKP = K::NKP, SFS = LPI * K::RS;
+  constexpr int WS = (T <= 32 && 32 % T == 0) ? 1 : 0;  // a line's threads share one warp
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
   C* twN = reinterpret_cast<C*>(smem_raw + K::OFF_TW);
@@ -862,8 +863,8 @@ k_zpass(const ZArgs<Tp> A) {
         if (s2 >= 0) r = cadd(r, cmuli_s(sb[s2 * LPI * NKP + k], sgn * (Tp)k));
         return r;
       });
-      fft.template run<+1>(v, j, sm, 1);
-      __syncthreads();  // the region doubles as exchange scratch: all reads done
+      fft.template run<+1, WS>(v, j, sm, 1);
+      F::template lsync<WS>();  // the region doubles as exchange scratch: all reads done
       C* dst = reinterpret_cast<C*>(myreg);
 #pragma unroll
       for (int m = 0; m < V; ++m) dst[j + T * m] = cscale(v[m], A.scale);
@@ -896,16 +897,17 @@ k_zpass(const ZArgs<Tp> A) {
       }
     }
     __syncthreads();
-    // ---- phase C: r2c of product `grp` (groups >= NOUT run idle for the barriers)
-    {
+    // ---- phase C: r2c of product `grp` (with block-wide line barriers, groups
+    // >= NOUT run idle for them; with line-level barriers they skip)
+    if (WS || grp < K::NOUT) {
       C v[V];
       const C* src = reinterpret_cast<const C*>(myreg);
 #pragma unroll
       for (int m = 0; m < V; ++m) v[m] = src[j + T * m];
-      fft.template run<-1>(v, j, sm, 1);
+      fft.template run<-1, WS>(v, j, sm, 1);
       C* out = A.ws + (grp < K::NOUT ? grp : 0) * fs + lo;
       const bool wr = ok && grp < K::NOUT;
-      r2c_post<F>(v, j, sm, 1, twN, [&](int k, C x) {
+      r2c_post<F, WS>(v, j, sm, 1, twN, [&](int k, C x) {
         if (wr) out[k] = x;
       });
     }
