@@ -584,23 +584,31 @@ def main():
     step_ach = step_alg / (ms_step * 1e-3) / 1e9
 
     # ---------------- end to end through the public API with host buffers ----------------
+    # every step: its state copied in from pinned host memory, one RK3 step,
+    # the result copied back to pinned host memory (sles.pipeline.HostStepper
+    # overlaps step k's copies with its neighbours' compute on two copy streams)
+    from sles.pipeline import HostStepper
     host_in = torch.empty(tuple(d.U_hat.shape), dtype=d.U_hat.dtype, pin_memory=True)
     host_out = torch.empty_like(host_in, pin_memory=True)
     host_in.copy_(d.U_hat)
     torch.cuda.synchronize()
     ke = max(10, args.steps // 4)
-
-    def e2e_step(dd):
-        dd.U_hat.copy_(host_in, non_blocking=True)
-        step(dd)
-        host_out.copy_(dd.U_hat, non_blocking=True)
-
-    e2e_step(d)
+    hs = HostStepper(d, steps=1)
+    hs.run(host_in, [host_out] * 2)
+    hs.synchronize()
     barrier()
-    e2e_secs = max_over_ranks(time_steps(d, ke, e2e_step))
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    hs.run(host_in, [host_out] * ke)
+    st.wait_stream(hs.d2h)  # the last device->host copy is inside the timed region
+    e1.record(st)
+    torch.cuda.synchronize()
+    e2e_secs = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     e2e_value = world * npts * ke / e2e_secs / 1e6
     io_bytes = host_in.numel() * host_in.element_size()
-    del host_in, host_out
+    del host_in, host_out, hs
 
     out = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
@@ -611,7 +619,9 @@ def main():
                       "parallelism": "replicas" if world > 1 else "single GPU", "autotune": tuned},
            "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": io_bytes,
                    "d2h_bytes_per_step": io_bytes, "steps": ke,
-                   "path": "domain.U_hat <- pinned host; RK3_method.solveForNextTimestep; pinned host <- U_hat"},
+                   "path": "sles.pipeline.HostStepper: per step pinned host -> U_hat, RK3_method."
+                           "solveForNextTimestep, U_hat -> pinned host; copies on two streams overlap the "
+                           "neighbouring steps' compute"},
            "gpu_launches": launches,
            "roofline": {"bound": "hbm", "kernel": "k_zpass (fused z pass: c2r x12, u x omega, Smagorinsky "
                                                   "stress, r2c x9)",
