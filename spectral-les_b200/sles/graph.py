@@ -62,11 +62,15 @@ class _Capture:
         side = [torch.cuda.Stream() for _ in self.domains]
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=main):
-            for d, s in zip(self.domains, side):
+            # fork every branch from the graph's start before joining any, so
+            # the members' launch sequences are independent (concurrent) nodes
+            for s in side:
                 s.wait_stream(main)
+            for d, s in zip(self.domains, side):
                 with torch.cuda.stream(s):
                     for _ in range(PERIOD):
                         _eager_step(d)
+            for s in side:
                 main.wait_stream(s)
         after = [_state_key(d) for d in self.domains]
         if after != before:
