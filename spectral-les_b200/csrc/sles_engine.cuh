@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 #include <mutex>
+#include <type_traits>
 #include <unordered_map>
 #include <unordered_set>
 
@@ -239,7 +240,13 @@ struct EngineImpl final : Engine {
 #endif
   // x pass: exchange padding divisor SLES_X_PADD (0: the plan's first radix)
   using FX = typename WithPad<typename PlanLo<Tp, N>::F, SLES_X_PADD>::F;
-  using FY = typename PlanLo<Tp, N>::F;
+  // per x-pass variant: the 32-byte-row tiles (XV 2) pad the exchange every 8 points
+  template <int XV>
+  using FXV = typename WithPad<typename PlanLo<Tp, N>::F, XV == 2 ? 8 : SLES_X_PADD>::F;
+#ifndef SLES_Y_PLANFOR
+#define SLES_Y_PLANFOR 0
+#endif
+  using FY = typename std::conditional<SLES_Y_PLANFOR != 0, typename PlanFor<Tp, N>::F, typename PlanLo<Tp, N>::F>::type;
   static constexpr int TZ = PlanFor<Tp, N / 2>::F::T;
   static constexpr int LPI = cmax(1, 16 / TZ);
 
@@ -248,7 +255,7 @@ struct EngineImpl final : Engine {
   }
   template <int XV>
   static int xchunks(const PlanInfo& p) {  // x-pass column chunks of variant XV
-    constexpr int WX = XGeo<Tp, N, FX, DIM, XV>::W;
+    constexpr int WX = XGeo<Tp, N, FXV<XV>, DIM, XV>::W;
     return (p.nk + WX - 1) / WX;
   }
   // x-pass variant used until a caller (the autotuner) sets another: the
@@ -336,7 +343,7 @@ struct EngineImpl final : Engine {
   }
   template <int LES, int PAR2D, int XV>
   int xpass_v(const PlanInfo& p, XArgs<Tp> a, cudaStream_t st) {
-    using K = XGeo<Tp, N, FX, DIM, XV>;
+    using K = XGeo<Tp, N, FXV<XV>, DIM, XV>;
     a.nchunks = xchunks<XV>(p);
     // state tiles the stage reads (ucur for viscous/forcing/update; u0 when
     // distinct from ucur; u1 = RK4 accumulator or ETD2's previous F1)
@@ -350,8 +357,8 @@ struct EngineImpl final : Engine {
     a.err = p.flags;
     const long long items = (long long)(DIM == 3 ? N : 1) * a.nchunks;
     if (a.kind == KX_ETD2P || a.kind == KX_ETD2C)
-      return launch_persistent(k_xpass<Tp, N, FX, DIM, LES, PAR2D, 1, XV>, items, K::THREADS, K::SMEM, st, a);
-    return launch_persistent(k_xpass<Tp, N, FX, DIM, LES, PAR2D, 0, XV>, items, K::THREADS, K::SMEM, st, a);
+      return launch_persistent(k_xpass<Tp, N, FXV<XV>, DIM, LES, PAR2D, 1, XV>, items, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_xpass<Tp, N, FXV<XV>, DIM, LES, PAR2D, 0, XV>, items, K::THREADS, K::SMEM, st, a);
   }
   int xpass_rt(const PlanInfo& p, const XArgs<Tp>& a, int les, int par2d, cudaStream_t st) {
     if (!les) return xpass<0, 0>(p, a, st);

@@ -180,7 +180,13 @@ __device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& 
 template <typename Tp, int N, class F, bool RING = true, int NBUF_SET = 0>
 struct TGeo {
   using C = typename CT<Tp>::C;
-  static constexpr int W = (sizeof(Tp) == 4) ? 8 : 4;       // 64-byte tile rows
+#ifndef SLES_Y_W
+#define SLES_Y_W 8
+#endif
+#ifndef SLES_Y_NBUF
+#define SLES_Y_NBUF 0
+#endif
+  static constexpr int W = (sizeof(Tp) == 4) ? SLES_Y_W : 4;  // 64-byte tile rows
   static constexpr int EPC = sizeof(C) / 8;                 // 8-byte tensor elements per complex
   static constexpr int T = F::T, V = F::V;
   static constexpr int THREADS = W * T;
@@ -188,7 +194,8 @@ struct TGeo {
   static constexpr int NBOX = N / RB;
   static constexpr int TE = N * W;                          // complex elements per tile
   static constexpr int NBUF =
-      NBUF_SET > 0 ? NBUF_SET : ((TE * sizeof(C) <= 16384) ? 4 : ((TE * sizeof(C) <= 32768) ? 3 : 2));
+      // 16 KB tiles: 4 buffers; larger tiles: 2 (at 512^3 a third 32 KB buffer made the y passes slower)
+      NBUF_SET > 0 ? NBUF_SET : (SLES_Y_NBUF > 0 ? SLES_Y_NBUF : ((TE * sizeof(C) <= 16384) ? 4 : 2));
   static constexpr unsigned BOX_BYTES = RB * W * sizeof(C);
   static constexpr int SCR = F::XLEN * W;
   using Ring = TileRing<C, NBUF, TE>;
@@ -220,13 +227,20 @@ struct XGeo {
   static constexpr int TE = N * W;
   static constexpr int SCR = F::XLEN * W;
   static constexpr int WARPS = (THREADS + 31) / 32;
-  static constexpr int TARGET = F32 ? (XV == 0 ? 16 : (XV == 1 ? 8 : 12)) : (XV == 2 ? 8 : WARPS);
+#ifndef SLES_X_T2
+#define SLES_X_T2 12
+#endif
+  static constexpr int TARGET = F32 ? (XV == 0 ? 16 : (XV == 1 ? 8 : SLES_X_T2)) : (XV == 2 ? 8 : WARPS);
   static constexpr int MINB0 = TARGET / WARPS;
   static constexpr int MINB = MINB0 < 1 ? 1 : (MINB0 > 16 ? 16 : MINB0);
   static constexpr size_t BASE = ((size_t)DIM * TE + SCR + N) * sizeof(C);  // + linear twiddle table
   // shared memory per block that keeps MINB blocks resident (228 KB per SM, 1 KB reserved per block)
   static constexpr size_t BUDGET = (228 / MINB - 1) * 1024;
-  static constexpr int NB = (XV == 0) ? 0 : ((BASE + 2 * (size_t)TE * sizeof(C) <= BUDGET) ? 2 : 0);
+#ifndef SLES_X_NB
+#define SLES_X_NB 2
+#endif
+  static constexpr int NB =
+      (XV == 0) ? 0 : ((BASE + (size_t)SLES_X_NB * TE * sizeof(C) <= BUDGET) ? SLES_X_NB : 0);
   static constexpr size_t SMEM = BASE + (size_t)NB * TE * sizeof(C);
 };
 
@@ -670,9 +684,12 @@ struct ZArgs {
   unsigned* err;         // error word (bounded-wait timeouts)
 };
 
+#ifndef SLES_Z_PADD
+#define SLES_Z_PADD 0
+#endif
 template <typename Tp, int N, int DIM, int LES, int PAR2D, int LPI>
 struct ZGeo {
-  using F = typename PlanFor<Tp, N / 2>::F;
+  using F = typename WithPad<typename PlanFor<Tp, N / 2>::F, SLES_Z_PADD>::F;
   using C = typename CT<Tp>::C;
   static constexpr int L = N / 2, T = F::T, V = F::V;
   static constexpr int NG = (DIM == 3) ? (LES ? 12 : 6) : (LES ? 6 : 3);    // physical fields
