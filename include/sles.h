@@ -241,6 +241,47 @@ int sles_adjoint_seed(sles_plan* plan, void* adj_ws, double dt, const void* ubar
 int sles_adjoint_prime(sles_plan* plan, void* adj_ws, const void* u_state, const void* lam, void* stream);
 int sles_adjoint_stage(sles_plan* plan, void* adj_ws, int stage, double dt, const void* u_next, void* ubar,
                        void* acc, void* lam, double* cs_grad, void* stream);
+/*
+ * Device-side time-step control (no host synchronisation per step): the
+ * driver loop of src/SM_solver.py:18-83 with its CFL rule (compute_dt,
+ * src/SM_solver.py:258-277) evaluated on the GPU.  The caller allocates this
+ * struct in device memory, fills it (umax_bits, flags, paused, nsteps and
+ * t_init zero) and passes it to sles_stage_ctl, which works as sles_stage with
+ * dt taken from it:
+ *  - stage 0's z pass reduces max_i max_x u_i of the state the step starts
+ *    from into umax_bits[parity] (find_max_velocity, src/SM_solver.py:245-255);
+ *  - a one-thread kernel then applies the reference's loop logic: dt =
+ *    min(CFL dx/u_max, 0.1 dx^2/nu) with CFL = cfl_first before the first
+ *    step and cfl after; t = dt before the first step; a step is taken only if
+ *    dt is finite and >= 1e-6, t < ek_next (else SLES_DT_SNAPSHOT: the caller
+ *    records E(k), raises ek_next and clears paused), and t < t_end and dt >=
+ *    1e-8 (else SLES_DT_DONE); a step taken adds dt to t and counts in nsteps;
+ *  - while paused, dt_step = 0 and every stage leaves the state unchanged.
+ * parity: the step's index modulo 2 (the z pass of a step collects into
+ * umax_bits[parity] while the kernel clears the other slot for the next step).
+ */
+typedef struct sles_dtctl {
+  double dt_step;                /* dt applied by the current step (0 while paused) */
+  double dt;                     /* last dt from the CFL rule */
+  double t;                      /* time as src/SM_solver.py counts it */
+  double t_end;                  /* final_time */
+  double ek_next;                /* next E(k) snapshot time */
+  double cfl_first, cfl;         /* CFL of the first step (0.3 in the reference) and later */
+  double dx, nu;
+  unsigned long long umax_bits[2];
+  unsigned flags;                /* SLES_DT_* */
+  unsigned paused;               /* non-zero: steps are no-ops */
+  unsigned nsteps;               /* steps taken */
+  unsigned t_init;               /* t was set to the first dt */
+  unsigned resumed;              /* set by the caller when it clears a snapshot pause: the next
+                                    step skips the snapshot test once (the reference takes at
+                                    most one snapshot per loop iteration) */
+  unsigned reserved;
+} sles_dtctl;
+enum { SLES_DT_DONE = 1, SLES_DT_SNAPSHOT = 2, SLES_DT_NAN = 4, SLES_DT_TOO_SMALL = 8 };
+int sles_stage_ctl(sles_plan* plan, int stage, void* dtctl, int parity, const void* u_cur, const void* u0,
+                   void* u1, void* u_out, void* aux_out, const void* u_phys, const void* curl_phys, int flags,
+                   void* stream);
 /* Human-readable text for a status code (static storage). */
 const char* sles_status_string(int status);
 int sles_version(void);

@@ -190,6 +190,17 @@ int sles_stage(sles_plan* p, int stage, double dt, const void* ucur, const void*
   return p->eng->stage(p->info, stage, dt, ucur, u0, u1, uout, aux, uphys, cphys, flags, (cudaStream_t)stream);
 }
 
+int sles_stage_ctl(sles_plan* p, int stage, void* dtctl, int parity, const void* ucur, const void* u0, void* u1,
+                   void* uout, void* aux, const void* uphys, const void* cphys, int flags, void* stream) {
+  if (int s = ready(p)) return s;
+  if (!dtctl || !ucur || !uout || (parity != 0 && parity != 1)) return SLES_ERR_INVALID_ARG;
+  if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
+  const int scheme = (flags & sles::STAGE_RK4) ? SLES_RK4 : p->info.d.scheme;
+  if ((scheme == SLES_RK4 && (!u0 || !u1)) || (scheme == SLES_RK3 && !u0)) return SLES_ERR_INVALID_ARG;
+  return p->eng->stage(p->info, stage, 0.0, ucur, u0, u1, uout, aux, uphys, cphys, flags, (cudaStream_t)stream,
+                       reinterpret_cast<sles_dtctl*>(dtctl), parity);
+}
+
 int sles_diag(sles_plan* p, const void* uh, const void* uphys, double* out, double* spectrum, int nshell,
               void* stream) {
   if (int s = ready(p)) return s;

@@ -51,7 +51,7 @@ struct Engine {
                   cudaStream_t st) = 0;
   virtual int stage(PlanInfo& p, int stage, double dt, const void* ucur, const void* u0, void* u1,
                     void* uout, void* aux, const void* uphys, const void* cphys, int flags,
-                    cudaStream_t st) = 0;
+                    cudaStream_t st, sles_dtctl* ctl = nullptr, int parity = 0) = 0;
   virtual int diag(PlanInfo& p, const void* uh, const void* uphys, double* out, double* spec, int nshell,
                    cudaStream_t st) = 0;
   virtual int profile_rhs(PlanInfo& p, const void* uh, void* du, int iters, double* ms, cudaStream_t st) = 0;
@@ -386,7 +386,8 @@ struct EngineImpl final : Engine {
   }
 
   template <int LES, int MODEL, int PAR2D>
-  int zpass(const PlanInfo& p, const Tp* uphys, const Tp* cphys, int stress_only, cudaStream_t st) {
+  int zpass(const PlanInfo& p, const Tp* uphys, const Tp* cphys, int stress_only, cudaStream_t st,
+            unsigned long long* umax) {
     using K = ZGeo<Tp, N, DIM, LES, PAR2D, LPI>;
     ZArgs<Tp> a{};
     a.ws = slot(p, 0);
@@ -402,22 +403,27 @@ struct EngineImpl final : Engine {
     a.rs = p.real_elems;
     a.stress_only = stress_only;
     a.err = p.flags;
+    a.umax = umax;
     if (p.nkp != K::NKP) return SLES_ERR_INVALID_ARG;
     return launch_persistent(k_zpass<Tp, N, DIM, LES, MODEL, PAR2D, LPI>, (a.nlines + LPI - 1) / LPI, K::THREADS, K::SMEM, st, a);
   }
   int zpass_rt(const PlanInfo& p, int les, int model, int par2d, const Tp* uphys, const Tp* cphys, int so,
-               cudaStream_t st) {
-    if (!les) return zpass<0, M_NONE, 0>(p, uphys, cphys, so, st);
+               cudaStream_t st, unsigned long long* umax = nullptr) {
+    if (!les) return zpass<0, M_NONE, 0>(p, uphys, cphys, so, st, umax);
     const int pz = (DIM == 2) ? par2d : 0;
     if (model == SLES_LES_SMAGORINSKY) {
-      return pz ? zpass<1, M_SMAG, 1>(p, uphys, cphys, so, st) : zpass<1, M_SMAG, 0>(p, uphys, cphys, so, st);
+      return pz ? zpass<1, M_SMAG, 1>(p, uphys, cphys, so, st, umax)
+                : zpass<1, M_SMAG, 0>(p, uphys, cphys, so, st, umax);
     }
-    return pz ? zpass<1, M_VREMAN, 1>(p, uphys, cphys, so, st) : zpass<1, M_VREMAN, 0>(p, uphys, cphys, so, st);
+    return pz ? zpass<1, M_VREMAN, 1>(p, uphys, cphys, so, st, umax)
+              : zpass<1, M_VREMAN, 0>(p, uphys, cphys, so, st, umax);
   }
 
-  // One RHS evaluation ending in the X pass described by `fin`.
+  // One RHS evaluation ending in the X pass described by `fin`.  ctl_step:
+  // the z pass collects max u into ctl_step->umax_bits[parity] and the
+  // time-step kernel runs before the X pass (stage 0 under device-side dt).
   int pipeline(const PlanInfo& p, int les, const C* ucur, bool primed, const Tp* uphys, const Tp* cphys,
-               int stress_only, XArgs<Tp> fin, cudaStream_t st) {
+               int stress_only, XArgs<Tp> fin, cudaStream_t st, sles_dtctl* ctl_step = nullptr, int parity = 0) {
     const int model = p.d.les_model, par2d = p.d.parity;
     if (!primed) {
       XArgs<Tp> a0 = xbase(p);
@@ -427,8 +433,10 @@ struct EngineImpl final : Engine {
       SLES_TRY(xpass_rt(p, a0, les, par2d, st));
     }
     SLES_TRY(les ? ypass<1>(p, 1, st) : ypass<0>(p, 1, st));
-    SLES_TRY(zpass_rt(p, les, model, par2d, uphys, cphys, stress_only, st));
+    SLES_TRY(zpass_rt(p, les, model, par2d, uphys, cphys, stress_only, st,
+                      ctl_step ? &ctl_step->umax_bits[parity & 1] : nullptr));
     SLES_TRY(les ? ypass<1>(p, 0, st) : ypass<0>(p, 0, st));
+    if (ctl_step) SLES_TRY(launch(k_dtctl, 1, 32, 0, st, ctl_step, parity & 1));
     fin.fwd = 1;
     return xpass_rt(p, fin, les, par2d, st);
   }
@@ -464,7 +472,8 @@ struct EngineImpl final : Engine {
   }
 
   int stage(PlanInfo& p, int s, double dt, const void* ucur, const void* u0, void* u1, void* uout, void* aux,
-            const void* uphys, const void* cphys, int flags, cudaStream_t st) override {
+            const void* uphys, const void* cphys, int flags, cudaStream_t st, sles_dtctl* ctl = nullptr,
+            int parity = 0) override {
     const auto& d = p.d;
     int les = d.les_model != SLES_LES_NONE;
     XArgs<Tp> a = xbase(p);
@@ -483,19 +492,19 @@ struct EngineImpl final : Engine {
       case SLES_RK4:
         if (s < 0 || s > 3) return SLES_ERR_INVALID_ARG;
         a.kind = KX_RK4;
-        a.c1 = (Tp)(rk4a[s] * dt);
-        a.c2 = (Tp)(s < 3 ? rk4b[s] * dt : 0.0);
+        a.m1 = rk4a[s];
+        a.m2 = s < 3 ? rk4b[s] : 0.0;
         break;
       case SLES_RK3:
         if (s < 0 || s > 2) return SLES_ERR_INVALID_ARG;
         if (d.parity) {
           a.kind = KX_RK3P;
-          if (s == 0) a.c2 = (Tp)(0.5 * dt);
-          if (s == 1) { a.c1 = (Tp)dt; a.c2 = (Tp)(2.0 * dt); }
-          if (s == 2) a.c1 = (Tp)dt;
+          if (s == 0) a.m2 = 0.5;
+          if (s == 1) { a.m1 = 1.0; a.m2 = 2.0; }
+          if (s == 2) a.m1 = 1.0;
         } else {
           a.kind = KX_SSP3;
-          a.c1 = (Tp)dt;
+          a.m1 = 1.0;
         }
         break;
       case SLES_ETD2:
@@ -510,6 +519,10 @@ struct EngineImpl final : Engine {
       default:
         return SLES_ERR_INVALID_ARG;
     }
+    // stage coefficients: the dt multiples, in float64 then rounded (device dt: the same products in-kernel)
+    a.c1 = (Tp)(a.m1 * dt);
+    a.c2 = (Tp)(a.m2 * dt);
+    if (ctl) a.dt_dev = &ctl->dt_step;
     if (flags & STAGE_RECORD_F1) {
       if (!aux) return SLES_ERR_INVALID_ARG;
       a.record_f1 = 1;
@@ -519,7 +532,8 @@ struct EngineImpl final : Engine {
         primed = false;
       }
     }
-    return pipeline(p, les, (const C*)ucur, primed, (const Tp*)uphys, (const Tp*)cphys, 0, a, st);
+    return pipeline(p, les, (const C*)ucur, primed, (const Tp*)uphys, (const Tp*)cphys, 0, a, st,
+                    (ctl && s == 0) ? ctl : nullptr, parity);
   }
 
   int profile_rhs(PlanInfo& p, const void* uh, void* du, int iters, double* ms, cudaStream_t st) override {

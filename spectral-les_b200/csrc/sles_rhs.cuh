@@ -66,7 +66,23 @@ struct XArgs {
   double kmax;
   Tp c1, c2;             // stage coefficients (host-computed in float64)
   double nu_d, dt_d;     // ETD2 weights are evaluated in float64
+  const double* dt_dev;  // non-null: dt read on the device (c1 = m1 dt, c2 = m2 dt, dt_d = dt)
+  double m1, m2;
 };
+
+// The stage's coefficients: host-computed, or from a device-side dt (adaptive
+// steps without host synchronisation; the products are the host's, in float64)
+template <typename Tp>
+struct StageCoef {
+  Tp c1, c2;
+  double dt;
+};
+template <typename Tp>
+__device__ __forceinline__ StageCoef<Tp> stage_coef(const XArgs<Tp>& A) {
+  if (!A.dt_dev) return StageCoef<Tp>{A.c1, A.c2, A.dt_d};
+  const double dt = *A.dt_dev;
+  return StageCoef<Tp>{(Tp)(A.m1 * dt), (Tp)(A.m2 * dt), dt};
+}
 
 // Per-position mask and projection for D velocity components (in place):
 // R <- mask * R, then R <- R - k (k . R)/|k|^2 (src/RK4_method.py:48-57);
@@ -99,7 +115,8 @@ __device__ __forceinline__ void project(const XArgs<Tp>& A, typename CT<Tp>::C (
 // ETD = 0 drops the exponential schemes (their float64 weights) from the
 // kernel, which keeps the Runge-Kutta kernels' register count down.
 template <typename Tp, int ETD>
-__device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& A, int c, typename CT<Tp>::C R,
+__device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& A, const StageCoef<Tp>& K, int c,
+                                                              typename CT<Tp>::C R,
                                                               typename CT<Tp>::C uc, typename CT<Tp>::C u0,
                                                               typename CT<Tp>::C u1, int k2, long long off) {
   using C = typename CT<Tp>::C;
@@ -113,25 +130,27 @@ __device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& 
   C un;
   if (ETD && (A.kind == KX_ETD2P || A.kind == KX_ETD2C)) {
     // parity: src/ETD2_method.py:16-29; corrected: Cox & Matthews (2002) eq. 22
-    const double z = A.dt_d * A.nu_d * (double)k2;
-    const double E = exp(-A.dt_d * A.nu_d * (double)k2);
+    const double z = K.dt * A.nu_d * (double)k2;
+    const double E = exp(-K.dt * A.nu_d * (double)k2);
     double w1, w0;
     if (A.kind == KX_ETD2P) {
       const double nk2 = A.nu_d * (double)k2;
-      const double den = (k2 == 0) ? 1.0 : A.dt_d * (nk2 * nk2);
+      const double den = (k2 == 0) ? 1.0 : K.dt * (nk2 * nk2);
       w1 = ((1.0 - z) + 2.0 * z) / den;
       w0 = (-E + 1.0 - z) / den;
     } else if (fabs(z) < 1e-2) {
-      const double h = A.dt_d;
+      const double h = K.dt;
       w1 = h * (1.5 - 2.0 * z / 3.0 + z * z / 4.0 - z * z * z / 15.0);
       w0 = h * (-0.5 + z / 6.0 - z * z / 24.0 + z * z * z / 120.0);
     } else {
-      const double h = A.dt_d;
+      const double h = K.dt;
       w1 = h * ((1.0 - z) * E - 1.0 + 2.0 * z) / (z * z);
       w0 = h * (-E + 1.0 - z) / (z * z);
     }
     un = cadd(cscale(uc, (Tp)E), cadd(cscale(R, (Tp)w1), cscale(u1, (Tp)w0)));
-    A.aux[o] = R;
+    // a paused step under device-side dt (dt = 0) passes the previous F1 through,
+    // so the two-step history is the same when the run resumes
+    A.aux[o] = (A.dt_dev && K.dt == 0.0) ? u1 : R;
     A.uout[o] = un;
     return un;
   }
@@ -139,30 +158,30 @@ __device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& 
   switch (A.kind) {
     case KX_RK4:  // RK4_method.py:20-27
       if (A.stage < 3) {
-        A.u1[o] = cadd(u1, cscale(dU, A.c1));
-        un = cadd(u0, cscale(dU, A.c2));
+        A.u1[o] = cadd(u1, cscale(dU, K.c1));
+        un = cadd(u0, cscale(dU, K.c2));
       } else {
-        un = cadd(u1, cscale(dU, A.c1));
+        un = cadd(u1, cscale(dU, K.c1));
         A.u1[o] = un;
       }
       break;
     case KX_RK3P:  // RK3_method.py:26-33
       if (A.stage == 0) {
-        un = cadd(u0, cscale(dU, A.c2));
+        un = cadd(u0, cscale(dU, K.c2));
       } else if (A.stage == 1) {
-        un = cadd(csub(u0, cscale(dU, A.c1)), cscale(dU, A.c2));
+        un = cadd(csub(u0, cscale(dU, K.c1)), cscale(dU, K.c2));
       } else {
         const C t = cadd(cadd(cscale(dU, (Tp)(1.0 / 6.0)), cscale(dU, (Tp)(2.0 / 3.0))), cscale(dU, (Tp)(1.0 / 6.0)));
-        un = cadd(u0, cscale(t, A.c1));
+        un = cadd(u0, cscale(t, K.c1));
       }
       break;
     case KX_SSP3:  // Shu & Osher (1988)
       if (A.stage == 0) {
-        un = cadd(u0, cscale(dU, A.c1));
+        un = cadd(u0, cscale(dU, K.c1));
       } else if (A.stage == 1) {
-        un = cadd(cscale(u0, (Tp)0.75), cscale(cadd(uc, cscale(dU, A.c1)), (Tp)0.25));
+        un = cadd(cscale(u0, (Tp)0.75), cscale(cadd(uc, cscale(dU, K.c1)), (Tp)0.25));
       } else {
-        un = cadd(cscale(u0, (Tp)(1.0 / 3.0)), cscale(cadd(uc, cscale(dU, A.c1)), (Tp)(2.0 / 3.0)));
+        un = cadd(cscale(u0, (Tp)(1.0 / 3.0)), cscale(cadd(uc, cscale(dU, K.c1)), (Tp)(2.0 / 3.0)));
       }
       break;
     default:  // KX_RHS
@@ -221,7 +240,10 @@ template <typename Tp, int N, class F, int DIM, int XV>
 struct XGeo {
   using C = typename CT<Tp>::C;
   static constexpr bool F32 = sizeof(Tp) == 4;
-  static constexpr int W = (XV == 2) ? (F32 ? 4 : 2) : (F32 ? 8 : 4);
+#ifndef SLES_X_W2
+#define SLES_X_W2 4
+#endif
+  static constexpr int W = (XV == 2) ? (F32 ? SLES_X_W2 : 2) : (F32 ? 8 : 4);
   static constexpr int T = F::T, V = F::V;
   static constexpr int THREADS = W * T;
   static constexpr int TE = N * W;
@@ -275,6 +297,7 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
   C* sm0 = rst + D * K::TE;                 // exchange scratch
   C* twt = sm0 + K::SCR;                    // twiddle table exp(-2 pi i e/N)
   C* ring = twt + N;                        // NB tile buffers [N][W]
+  const StageCoef<Tp> SC = stage_coef<Tp>(A);
   const int tid = threadIdx.x;
   const int l = tid % W, j = tid / W;
   F::fill_table_lin(twt);
@@ -456,7 +479,7 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
             u0m = A.need_u0 ? A.u0[c * fs + off] : ucm;
             u1m = A.need_u1 ? A.u1[c * fs + off] : cmk<C>(0, 0);
           }
-          v[m] = update_component<Tp, ETD>(A, c, rst[rpos(c, m)], ucm, u0m, u1m, k2, off);
+          v[m] = update_component<Tp, ETD>(A, SC, c, rst[rpos(c, m)], ucm, u0m, u1m, k2, off);
         }
       } else {
 #pragma unroll
@@ -682,7 +705,42 @@ struct ZArgs {
   long long rs;          // elements per real field
   int stress_only;       // 1: drop u x omega (evaluates the LES stress alone)
   unsigned* err;         // error word (bounded-wait timeouts)
+  unsigned long long* umax;  // non-null: max over components and points of u (ordered encoding)
 };
+
+// order-preserving encoding of a double as an unsigned 64-bit integer (for atomicMax)
+__device__ __forceinline__ unsigned long long ord_encode(double x) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double ord_decode(unsigned long long e) {
+  const unsigned long long u = (e >> 63) ? (e & 0x7fffffffffffffffull) : ~e;
+  return __longlong_as_double((long long)u);
+}
+
+// One step of the driver loop's time-step logic (src/SM_solver.py:18-83,
+// compute_dt :258-277) on the device; see sles_dtctl in include/sles.h.
+static __global__ void k_dtctl(sles_dtctl* c, int parity) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double umax = c->umax_bits[parity] ? ord_decode(c->umax_bits[parity]) : -INFINITY;
+  c->umax_bits[parity ^ 1] = 0ull;  // the next step collects from scratch
+  c->dt_step = 0.0;
+  if (c->paused) return;
+  const double cfl = (c->nsteps == 0) ? c->cfl_first : c->cfl;
+  const double dt1 = cfl * c->dx / umax;
+  const double dt2 = (c->nu > 0.0) ? 0.1 * c->dx * c->dx / c->nu : 1e6;
+  const double dt = fmin(dt1, dt2);
+  if (!(dt == dt)) { c->flags |= SLES_DT_NAN; c->paused = 1; return; }
+  if (dt < 1e-6) { c->flags |= SLES_DT_TOO_SMALL; c->paused = 1; return; }
+  c->dt = dt;
+  if (c->nsteps == 0 && !c->t_init) { c->t = dt; c->t_init = 1; }
+  if (c->t >= c->ek_next && !c->resumed) { c->flags |= SLES_DT_SNAPSHOT; c->paused = 1; return; }
+  c->resumed = 0;
+  if (c->t >= c->t_end || dt < 1e-8) { c->flags |= SLES_DT_DONE; c->paused = 1; return; }
+  c->t += dt;
+  c->dt_step = dt;
+  c->nsteps += 1;
+}
 
 #ifndef SLES_Z_PADD
 #define SLES_Z_PADD 0
@@ -704,6 +762,7 @@ struct ZGeo {
   static constexpr int LS = ((F::XLEN + 15) / 16) * 16 + 8;
   static constexpr int RS = 2 * LS;
   static_assert(RS >= N, "region must hold a physical line");
+  static_assert((size_t)NG * LPI * RS * sizeof(Tp) >= (size_t)THREADS * sizeof(double), "regions hold the u_max partials");
   static constexpr int STAGE = NIN * LPI * NKP;   // complex elements per staging buffer
   static constexpr size_t OFF_TW = 16;
   static constexpr size_t OFF_STAGE = OFF_TW + (size_t)L * sizeof(C);
@@ -860,6 +919,7 @@ k_zpass(const ZArgs<Tp> A) {
       bulk_g2s(stage + buf * K::STAGE + s * LPI * NKP, A.ws + s * fs + l0 * A.nkp, bytes, &bar[buf]);
   };
   if (tid == 0 && blockIdx.x < nbi) issue(blockIdx.x, 0);
+  double lmax = -INFINITY;  // max of u over this thread's points (when A.umax)
   int iter = 0;
   for (long long bi = blockIdx.x; bi < nbi; bi += gridDim.x, ++iter) {  // persistent over line groups
     const int buf = iter & 1;
@@ -907,6 +967,10 @@ k_zpass(const ZArgs<Tp> A) {
         co = cb;
       }
       const int sp = pln * K::RS + z;
+      if (A.umax) {
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) lmax = fmax(lmax, (double)(uo ? uo[c] : reg[c * SFS + sp]));
+      }
       z_pointwise<Tp, DIM, LES, MODEL, PAR2D>(reg, SFS, sp, uo, co, A.cdx2);
       if (A.stress_only) {
 #pragma unroll
@@ -927,6 +991,17 @@ k_zpass(const ZArgs<Tp> A) {
       r2c_post<F, WS>(v, j, sm, 1, twN, [&](int k, C x) {
         if (wr) out[k] = x;
       });
+    }
+  }
+  if (A.umax) {  // block maximum through the (now idle) line regions, one atomic per block
+    __syncthreads();
+    double* part = reinterpret_cast<double*>(reg);  // THREADS doubles fit in the regions
+    part[tid] = lmax;
+    __syncthreads();
+    if (tid == 0) {
+      double m = -INFINITY;
+      for (int w = 0; w < K::THREADS; ++w) m = fmax(m, part[w]);
+      atomicMax(A.umax, ord_encode(m));
     }
   }
 }

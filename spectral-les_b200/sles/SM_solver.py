@@ -51,7 +51,15 @@ def _step(domain):
         raise ValueError("Invalid method name")
 
 
-def spectralMethodSolver(domain, file_out_time: float = 0.0, No_Ek_plot: int = 5, verbose: bool = True):
+def spectralMethodSolver(domain, file_out_time: float = 0.0, No_Ek_plot: int = 5, verbose: bool = True,
+                         device_dt: bool = False, chunk: int = 32):
+    """src/SM_solver.py:18-83.  device_dt=True runs the same loop with the
+    time-step logic on the GPU (u_max reduced inside the fused z pass, dt and t
+    kept in device memory) and the steps replayed as CUDA graphs of ``chunk``
+    steps; the host synchronises once per chunk and at each E(k) snapshot,
+    giving the same steps, dt sequence and snapshots as the host loop."""
+    if device_dt:
+        return _solver_device_dt(domain, No_Ek_plot, verbose, chunk)
     d = domain
     u_max = max_velocity(d)
     d.dt = compute_dt(None, u_max, d.nu, dx=d.dx, CFL=0.3)
@@ -79,6 +87,65 @@ def spectralMethodSolver(domain, file_out_time: float = 0.0, No_Ek_plot: int = 5
                 print("\n############ dt = Nan #############\n", counter)
             break
         counter += 1
+    if columns:
+        import pandas as pd
+        pd.DataFrame(columns).to_csv("Ek_plot_data.csv", index=False)
+    total = time.time() - start
+    if verbose and counter > 0:
+        print(f"=>  run time: {total} sec")
+        print(f"Time per gridpoint per timestep: {total * d.num_processes / (d.N ** d.dim * counter)}\n")
+    return counter
+
+
+def _solver_device_dt(d, No_Ek_plot, verbose, chunk):
+    import torch
+
+    from . import _native as nat
+    from .graph import CapturedStepper
+    Ek_interval = d.T / No_Ek_plot if No_Ek_plot != 0 else 0
+    c = nat.DtCtl()
+    c.t_end, c.cfl_first, c.cfl, c.dx, c.nu = d.T, 0.3, d.CFL, d.dx, d.nu
+    start = time.time()
+    d.U_hat1[...] = d.U_hat            # src/SM_solver.py:33
+    columns = {}
+    Ek_counter = 0.0
+    if Ek_interval > 0:                # the first iteration's snapshot (t = dt_0 >= 0), taken here so
+        tk, tE = reference_binned_spectrum(d)  # that the first device step is never a paused one
+        t0 = compute_dt(None, max_velocity(d), d.nu, dx=d.dx, CFL=0.3)
+        columns[f"k-{t0:g}"] = tk
+        columns[f"Ek-{t0:g}"] = tE
+        Ek_counter += Ek_interval
+    c.ek_next = Ek_counter if Ek_interval > 0 else float("inf")
+    c.resumed = 1 if Ek_interval > 0 else 0
+    ctl = torch.frombuffer(bytearray(bytes(c)), dtype=torch.uint8).to(d.device)
+    d._dtctl, d._parity = ctl, 0
+    stepper = CapturedStepper(d)
+    try:
+        while True:
+            stepper.advance(chunk)
+            st = nat.DtCtl.from_buffer_copy(bytes(ctl.cpu().numpy()))
+            if st.flags & nat.DT_SNAPSHOT:
+                tk, tE = reference_binned_spectrum(d)
+                columns[f"k-{st.t:g}"] = tk
+                columns[f"Ek-{st.t:g}"] = tE
+                Ek_counter += Ek_interval
+                st.ek_next, st.flags, st.paused, st.resumed = Ek_counter, st.flags & ~nat.DT_SNAPSHOT, 0, 1
+                ctl.copy_(torch.frombuffer(bytearray(bytes(st)), dtype=torch.uint8))
+                continue
+            if st.flags & nat.DT_NAN:
+                if verbose:
+                    print("\n############ dt = Nan #############\n", st.nsteps)
+                break
+            if st.flags & nat.DT_TOO_SMALL:
+                print(f"\n\n ###  Time step (dt = {st.dt:g}) is smaller than 1e-6  ###\n\n")
+                raise SystemExit(1)
+            if st.flags & nat.DT_DONE:
+                break
+    finally:
+        torch.cuda.synchronize(d.device)
+        d._dtctl = None
+    d.dt = st.dt
+    counter = st.nsteps
     if columns:
         import pandas as pd
         pd.DataFrame(columns).to_csv("Ek_plot_data.csv", index=False)

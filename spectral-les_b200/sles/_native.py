@@ -26,8 +26,19 @@ EXPORTED = [
     "sles_velocity_curl", "sles_velocity_gradient", "sles_rhs", "sles_stage", "sles_diag",
     "sles_status_string", "sles_version", "sles_profile_rhs", "sles_rhs_static_workspace",
     "sles_adjoint_workspace_bytes", "sles_adjoint_seed", "sles_adjoint_prime", "sles_adjoint_stage",
-    "sles_plan_variant_count", "sles_plan_get_variant", "sles_plan_set_variant",
+    "sles_plan_variant_count", "sles_plan_get_variant", "sles_plan_set_variant", "sles_stage_ctl",
 ]
+DT_DONE, DT_SNAPSHOT, DT_NAN, DT_TOO_SMALL = 1, 2, 4, 8
+
+
+class DtCtl(ctypes.Structure):
+    """sles_dtctl (include/sles.h): device-side time-step control."""
+    _fields_ = [("dt_step", ctypes.c_double), ("dt", ctypes.c_double), ("t", ctypes.c_double),
+                ("t_end", ctypes.c_double), ("ek_next", ctypes.c_double), ("cfl_first", ctypes.c_double),
+                ("cfl", ctypes.c_double), ("dx", ctypes.c_double), ("nu", ctypes.c_double),
+                ("umax_bits", ctypes.c_uint64 * 2), ("flags", ctypes.c_uint32), ("paused", ctypes.c_uint32),
+                ("nsteps", ctypes.c_uint32), ("t_init", ctypes.c_uint32), ("resumed", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 PASS_X = 0
 
 
@@ -80,6 +91,7 @@ def load_library(path: str = LIB_PATH):
         "sles_profile_rhs": (i, [vp, vp, vp, i, vp, vp]),
         "sles_rhs_static_workspace": (i, [vp, vp, vp, vp, vp, vp, vp]),
         "sles_version": (i, []),
+        "sles_stage_ctl": (i, [vp, i, vp, i, vp, vp, vp, vp, vp, vp, vp, i, vp]),
         "sles_plan_variant_count": (i, [vp, i]),
         "sles_plan_get_variant": (i, [vp, i]),
         "sles_plan_set_variant": (i, [vp, i, i]),
@@ -180,6 +192,13 @@ class Plan:
     def stage(self, stage, dt, ucur, u0, u1, uout, aux=None, uphys=None, cphys=None, flags=0):
         check(self.L.sles_stage(self.h, int(stage), float(dt), ptr(ucur), ptr(u0), ptr(u1), ptr(uout), ptr(aux),
                                 ptr(uphys), ptr(cphys), int(flags), stream_handle(self.device)), "sles_stage")
+
+    def stage_ctl(self, stage, ctl, parity, ucur, u0, u1, uout, aux=None, uphys=None, cphys=None, flags=0):
+        """As stage(), with dt from the device-side controller ``ctl`` (a uint8
+        device tensor holding a DtCtl)."""
+        check(self.L.sles_stage_ctl(self.h, int(stage), ptr(ctl), int(parity), ptr(ucur), ptr(u0), ptr(u1), ptr(uout),
+                                    ptr(aux), ptr(uphys), ptr(cphys), int(flags), stream_handle(self.device)),
+              "sles_stage_ctl")
 
     def profile_rhs(self, uh, du, iters):
         """Mean ms per launch of {x-inverse, y-inverse, z, y-forward, x-forward}."""

@@ -25,7 +25,10 @@ def stage(d, k, dt, ucur, u0, u1, uout, aux=None, flags=0, first=False):
         uphys, cphys = d._phys_override()
     primed = d._primed == _key(ucur)
     f = flags | (nat.STAGE_PRIMED if primed else 0)
-    d._plan.stage(k, dt, ucur, u0, u1, uout, aux, uphys, cphys, f)
+    if d._dtctl is not None:  # dt from the device-side controller (SM_solver device mode)
+        d._plan.stage_ctl(k, d._dtctl, d._parity, ucur, u0, u1, uout, aux, uphys, cphys, f)
+    else:
+        d._plan.stage(k, dt, ucur, u0, u1, uout, aux, uphys, cphys, f)
     LAUNCHES[0] += (4 if d.dim == 3 else 2) + (0 if primed else 1)
     d._primed = None if (flags & nat.STAGE_NO_PREPARE) else _key(uout)
 
@@ -41,6 +44,7 @@ def rk4_step(d, record_f1=False):
         stage(d, rk, dt, ucur, A, C, B, aux, flags, first=(rk == 0))
     d._s_uhat, d._s_u0 = B, A
     d._mark_stepped()
+    d._parity ^= 1
 
 
 def rk3_step(d):
@@ -51,6 +55,7 @@ def rk3_step(d):
         stage(d, rk, dt, A if rk == 0 else B, A, None, B, first=(rk == 0))
     d._s_uhat, d._s_u0 = B, A
     d._mark_stepped()
+    d._parity ^= 1
 
 
 def etd2_step(d):
@@ -76,6 +81,7 @@ def etd2_step(d):
     stage(d, 0, d.dt, U, None, d._s_f1, U, d._s_f0, 0, first=True)
     d._s_f0, d._s_f1 = d._s_f1, d._s_f0
     d._mark_stepped()
+    d._parity ^= 1
 
 
 def compute_rhs(d, dU, rk):

@@ -33,7 +33,8 @@ def _eager_step(d):
 def _state_key(d):
     """Buffer roles, workspace priming and baked-in parameters of a domain."""
     roles = tuple(None if s is None else s.data_ptr() for s in (d._s_uhat, d._s_u0, d._s_u1, d._s_f0, d._s_f1))
-    return roles, d._primed, (d.dt, d.nu, d.Cs, d.forcing), d.firstIteration
+    ctl = None if d._dtctl is None else d._dtctl.data_ptr()
+    return roles, d._primed, (d.dt, d.nu, d.Cs, d.forcing), d.firstIteration, ctl, d._parity
 
 
 class _Capture:

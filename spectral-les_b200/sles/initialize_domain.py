@@ -168,6 +168,8 @@ class InitializeDomain:
         self._phys_user = False        # U/curl were set by a setter: stage 0 must use them
         self._phys_ver = (self._U._version, self._curl._version)
         self._primed = None            # (storage data_ptr, version) whose x-inverse sits in the workspace
+        self._dtctl = None             # device-side dt controller (SM_solver device mode), else None
+        self._parity = 0               # step index mod 2 (the controller's u_max slot)
         self._lazy = {}
 
     # ------------------------------------------------------------------ storage
