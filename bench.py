@@ -158,12 +158,8 @@ def spectrum_error(a, b, n, floor=1e-8):
     ea, eb = shell_spectrum(a, n, kc + 1)[1:], shell_spectrum(b, n, kc + 1)[1:]
     r = (ea - eb).abs() / eb
     live = eb >= floor * eb.max()
-    klast = int(torch_nonzero_last(live)) + 1
+    klast = int(live.nonzero().max()) + 1
     return float(r[live].max()), klast, float(r.max())
-
-
-def torch_nonzero_last(mask):
-    return mask.nonzero().max()
 
 
 def tune_domain(d):
@@ -565,6 +561,7 @@ def main():
     with ClockSampler(gpu_index()) as clk:
         secs = time_steps(d, args.steps, step)
     launches = _stepper.LAUNCHES[0]
+    d._plan.check()  # no bounded wait gave up during the timed steps
     secs = max_over_ranks(secs)
     value = world * npts * args.steps / secs / 1e6
     ms_step = secs / args.steps * 1e3

@@ -282,6 +282,19 @@ enum { SLES_DT_DONE = 1, SLES_DT_SNAPSHOT = 2, SLES_DT_NAN = 4, SLES_DT_TOO_SMAL
 int sles_stage_ctl(sles_plan* plan, int stage, void* dtctl, int parity, const void* u_cur, const void* u0,
                    void* u1, void* u_out, void* aux_out, const void* u_phys, const void* curl_phys, int flags,
                    void* stream);
+/*
+ * Device error word of the plan's workspace (no counterpart in the reference).
+ * Kernels never spin without bound: a wait that gives up (e.g. on an mbarrier
+ * a TMA copy should have completed) sets a bit in the word and the kernel
+ * returns.  sles_plan_check synchronises `stream`, stores the word in
+ * *flags_out (may be NULL), clears it and returns SLES_ERR_TIMEOUT /
+ * SLES_ERR_NONFINITE when such a bit was set, else SLES_OK.
+ * sles_selftest_wait_timeout enqueues a kernel that waits on an mbarrier
+ * nothing arrives at, with a short limit, to exercise that path (the CUDA
+ * context stays usable).
+ */
+int sles_plan_check(sles_plan* plan, unsigned* flags_out, void* stream);
+int sles_selftest_wait_timeout(sles_plan* plan, void* stream);
 /* Human-readable text for a status code (static storage). */
 const char* sles_status_string(int status);
 int sles_version(void);

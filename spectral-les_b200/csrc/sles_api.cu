@@ -201,6 +201,25 @@ int sles_stage_ctl(sles_plan* p, int stage, void* dtctl, int parity, const void*
                        reinterpret_cast<sles_dtctl*>(dtctl), parity);
 }
 
+int sles_plan_check(sles_plan* p, unsigned* flags_out, void* stream) {
+  if (int s = ready(p)) return s;
+  unsigned w = 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(&w, p->info.flags, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return SLES_ERR_CUDA;
+  if (flags_out) *flags_out = w;
+  if (w && cudaMemsetAsync(p->info.flags, 0, sizeof(unsigned), st) != cudaSuccess) return SLES_ERR_CUDA;
+  if (w & sles::SLES_ERRF_WAIT_TIMEOUT) return SLES_ERR_TIMEOUT;
+  if (w & sles::SLES_ERRF_NONFINITE) return SLES_ERR_NONFINITE;
+  return SLES_OK;
+}
+
+int sles_selftest_wait_timeout(sles_plan* p, void* stream) {
+  if (int s = ready(p)) return s;
+  return sles::launch(sles::k_wait_selftest, 1, 32, 0, (cudaStream_t)stream, p->info.flags, 4096L);
+}
+
 int sles_diag(sles_plan* p, const void* uh, const void* uphys, double* out, double* spectrum, int nshell,
               void* stream) {
   if (int s = ready(p)) return s;

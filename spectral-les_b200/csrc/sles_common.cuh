@@ -81,11 +81,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   return ok != 0;
 }
 
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned* flag) {
-  for (long it = 0; it < MBAR_SPIN_LIMIT; ++it)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned* flag,
+                                                  long limit = MBAR_SPIN_LIMIT) {
+  for (long it = 0; it < limit; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   raise_flag(flag, SLES_ERRF_WAIT_TIMEOUT);
   return false;
+}
+
+// Self-test of the timeout path: waits on an mbarrier that nothing arrives
+// at; the bounded wait gives up after `limit` polls and raises the flag.
+static __global__ void k_wait_selftest(unsigned* flag, long limit) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_wait_bounded(&bar, 0, flag, limit);
 }
 
 // bytes must be a multiple of 16; both addresses 16-byte aligned

@@ -322,17 +322,6 @@ struct EngineImpl final : Engine {
     return a;
   }
 
-  // x-pass tile map over `nslot` fields starting at base
-  int xmap(const PlanInfo& p, CUtensorMap* m, const void* base, int nslot) const {
-    using K = TGeo<Tp, N, FX>;
-    const long long cb = sizeof(C);
-    if (DIM == 3)
-      return make_tmap(m, base, K::EPC, p.nk, N, (long long)N * p.nkp * cb, N, (long long)p.nkp * cb, nslot,
-                       p.hc_elems * cb, K::W, K::RB);
-    return make_tmap(m, base, K::EPC, p.nk, N, (long long)p.nkp * cb, 1, (long long)N * p.nkp * cb, nslot,
-                     p.hc_elems * cb, K::W, K::RB);
-  }
-
   template <int LES, int PAR2D>
   int xpass(const PlanInfo& p, XArgs<Tp> a, cudaStream_t st) {
     switch (p.xvar) {

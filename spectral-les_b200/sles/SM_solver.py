@@ -87,6 +87,7 @@ def spectralMethodSolver(domain, file_out_time: float = 0.0, No_Ek_plot: int = 5
                 print("\n############ dt = Nan #############\n", counter)
             break
         counter += 1
+    d._plan.check()  # a kernel's bounded wait that gave up raises here
     if columns:
         import pandas as pd
         pd.DataFrame(columns).to_csv("Ek_plot_data.csv", index=False)
@@ -146,6 +147,7 @@ def _solver_device_dt(d, No_Ek_plot, verbose, chunk):
         d._dtctl = None
     d.dt = st.dt
     counter = st.nsteps
+    d._plan.check()  # a kernel's bounded wait that gave up raises here
     if columns:
         import pandas as pd
         pd.DataFrame(columns).to_csv("Ek_plot_data.csv", index=False)

@@ -27,6 +27,7 @@ EXPORTED = [
     "sles_status_string", "sles_version", "sles_profile_rhs", "sles_rhs_static_workspace",
     "sles_adjoint_workspace_bytes", "sles_adjoint_seed", "sles_adjoint_prime", "sles_adjoint_stage",
     "sles_plan_variant_count", "sles_plan_get_variant", "sles_plan_set_variant", "sles_stage_ctl",
+    "sles_plan_check", "sles_selftest_wait_timeout",
 ]
 DT_DONE, DT_SNAPSHOT, DT_NAN, DT_TOO_SMALL = 1, 2, 4, 8
 
@@ -92,6 +93,8 @@ def load_library(path: str = LIB_PATH):
         "sles_rhs_static_workspace": (i, [vp, vp, vp, vp, vp, vp, vp]),
         "sles_version": (i, []),
         "sles_stage_ctl": (i, [vp, i, vp, i, vp, vp, vp, vp, vp, vp, vp, i, vp]),
+        "sles_plan_check": (i, [vp, ctypes.POINTER(ctypes.c_uint), vp]),
+        "sles_selftest_wait_timeout": (i, [vp, vp]),
         "sles_plan_variant_count": (i, [vp, i]),
         "sles_plan_get_variant": (i, [vp, i]),
         "sles_plan_set_variant": (i, [vp, i, i]),
@@ -141,7 +144,9 @@ class Plan:
         self.hc_elems, self.real_elems, self.nkp, self.nk = lay.hc_elems, lay.real_elems, lay.nkp, lay.nk
         nbytes = int(L.sles_plan_workspace_bytes(h))
         with torch.cuda.device(self.device):
-            self.workspace = torch.empty(nbytes + 256, dtype=torch.uint8, device=self.device)
+            # zeroed: the header's error word must start clear (the caching
+            # allocator may hand back memory holding another tensor's bytes)
+            self.workspace = torch.zeros(nbytes + 256, dtype=torch.uint8, device=self.device)
         off = (-self.workspace.data_ptr()) % 256
         self._ws_ptr = self.workspace.data_ptr() + off
         check(L.sles_plan_set_workspace(h, ctypes.c_void_p(self._ws_ptr), ctypes.c_size_t(nbytes)),
@@ -199,6 +204,16 @@ class Plan:
         check(self.L.sles_stage_ctl(self.h, int(stage), ptr(ctl), int(parity), ptr(ucur), ptr(u0), ptr(u1), ptr(uout),
                                     ptr(aux), ptr(uphys), ptr(cphys), int(flags), stream_handle(self.device)),
               "sles_stage_ctl")
+
+    def check(self):
+        """Synchronise this plan's stream and raise SlesError if a kernel's
+        bounded wait gave up (the device error word is cleared)."""
+        w = ctypes.c_uint(0)
+        check(self.L.sles_plan_check(self.h, ctypes.byref(w), stream_handle(self.device)), "sles_plan_check")
+        return int(w.value)
+
+    def selftest_wait_timeout(self):
+        check(self.L.sles_selftest_wait_timeout(self.h, stream_handle(self.device)), "sles_selftest_wait_timeout")
 
     def profile_rhs(self, uh, du, iters):
         """Mean ms per launch of {x-inverse, y-inverse, z, y-forward, x-forward}."""

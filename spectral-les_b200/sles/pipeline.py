@@ -85,3 +85,4 @@ class HostStepper:
         torch.cuda.current_stream(self.d.device).synchronize()
         self.d2h.synchronize()
         self.h2d.synchronize()
+        self.d._plan.check()
