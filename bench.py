@@ -434,6 +434,39 @@ def bench_adjoint(rank):
     return out
 
 
+def bench_driver(rank, n=128, t_end=4.0):
+    """The driver loop (SM_solver.spectralMethodSolver, adaptive CFL dt, E(k)
+    snapshots) with its time-step logic on the host (a device->host read of
+    max u every step) against device_dt=True (dt on the GPU, steps replayed as
+    graph chunks): 128^3 FP32 Smagorinsky, reference RK3, CFL 0.5, wall time."""
+    import tempfile
+    import torch
+    from sles.SM_solver import spectralMethodSolver
+    out = {}
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as td:
+        os.chdir(td)
+        try:
+            for mode in (False, True, False, True):  # the first pair warms up
+                d = make_domain(n, "float32", rank)
+                d.T, d.CFL = t_end, 0.5
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                steps = spectralMethodSolver(d, No_Ek_plot=5, verbose=False, device_dt=mode, chunk=32)
+                torch.cuda.synchronize()
+                secs = time.perf_counter() - t0
+                out["device_dt" if mode else "host_dt"] = {
+                    "steps": steps, "wall_s": round(secs, 4), "final_dt": d.dt,
+                    "value": round(float(n) ** 3 * steps / secs / 1e6, 2), "unit": UNIT}
+                del d
+        finally:
+            os.chdir(cwd)
+    out["speedup_device_dt"] = round(out["device_dt"]["value"] / out["host_dt"]["value"], 3)
+    out["config"] = ("%d^3 FP32 Smagorinsky Cs=0.17, reference RK3, nu=1e-4, CFL 0.5 (0.3 first step), final "
+                     "time %g, 5 E(k) snapshots; wall time of spectralMethodSolver including its set-up" % (n, t_end))
+    return out
+
+
 def ensemble_members(seed):
     """48 members from one generator: 32 2D vorticity runs (N in {256, 512,
     1024}, nu log-uniform in [1e-5, 1e-3], Gaussian vorticity peaked at k=10,
@@ -507,7 +540,7 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (use the default or cached kernel variants)")
-    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble"],
+    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble", "driver"],
                     help="run one extra block alone and print it (profiling; not a bench line)")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference", "at least 3 warm-up steps"
@@ -547,7 +580,7 @@ def main():
     if args.only:
         peak, _ = measured_peak()
         fn = {"n512": lambda: bench_512(peak, rank), "adjoint": lambda: bench_adjoint(rank),
-              "ensemble": lambda: bench_ensemble(rank)}[args.only]
+              "ensemble": lambda: bench_ensemble(rank), "driver": lambda: bench_driver(rank)}[args.only]
         print(json.dumps({"only": args.only, "result": fn()}))
         return
 
@@ -662,6 +695,7 @@ def main():
         out["adjoint"] = adj
         out["adjoint_fwd_ratio"] = adj["adjoint_fwd_ratio"]
         out["ensemble"] = bench_ensemble(rank)
+        out["driver_loop"] = bench_driver(rank)
     else:
         out["adjoint_fwd_ratio"] = None
 

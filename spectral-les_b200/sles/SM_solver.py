@@ -121,10 +121,17 @@ def _solver_device_dt(d, No_Ek_plot, verbose, chunk):
     ctl = torch.frombuffer(bytearray(bytes(c)), dtype=torch.uint8).to(d.device)
     d._dtctl, d._parity = ctl, 0
     stepper = CapturedStepper(d)
+    n_next = chunk
     try:
         while True:
-            stepper.advance(chunk)
+            stepper.advance(n_next)
             st = nat.DtCtl.from_buffer_copy(bytes(ctl.cpu().numpy()))
+            # next chunk: about the steps left before the next snapshot or the
+            # end at the current dt (a chunk that overshoots runs paused no-op steps)
+            nxt = min(st.ek_next, st.t_end) - st.t
+            est = int(nxt / st.dt) + 1 if st.dt > 0 and nxt == nxt else chunk
+            n_next = max(2, min(chunk, est))
+            n_next += n_next % 2
             if st.flags & nat.DT_SNAPSHOT:
                 tk, tE = reference_binned_spectrum(d)
                 columns[f"k-{st.t:g}"] = tk
