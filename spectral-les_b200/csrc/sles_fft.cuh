@@ -240,7 +240,7 @@ struct LineFFT {
       if (Ns > 1) {  // tab points at this stage's [r-1][k] table (Ns entries per r)
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          const C w = LIN ? tab[k * r * (L / (Ns * R))] : tab[(r - 1) * Ns + k];
+          const C w = LIN ? tab[lin_pad(k * r * (L / (Ns * R)))] : tab[(r - 1) * Ns + k];
           u[r] = (DIR < 0) ? cmul(u[r], w) : cmulc(u[r], w);
         }
       }
@@ -289,8 +289,12 @@ struct LineFFT {
 
   // linear table W_L^e, e < L (float64, rounded once)
   __device__ __forceinline__ static void fill_table_lin(C* tab) {
-    for (int e = threadIdx.x; e < L; e += blockDim.x) tab[e] = twiddle<Tp>(e, L, -1);
+    for (int e = threadIdx.x; e < L; e += blockDim.x) tab[lin_pad(e)] = twiddle<Tp>(e, L, -1);
   }
+  // The linear table is read at strides k*r*L/(Ns*R); one pad slot per 16
+  // entries spreads the indices a warp reads over the shared-memory banks.
+  static constexpr int LIN_LEN = L + L / 16 + 1;  // slots of the padded linear table
+  __device__ __forceinline__ static int lin_pad(int e) { return e + (int)((unsigned)e / 16u); }
 
   // cooperative fill of the per-stage twiddle tables (TAB entries; float64, rounded once)
   __device__ __forceinline__ static void fill_table(C* tab) {

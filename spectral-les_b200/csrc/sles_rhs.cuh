@@ -255,7 +255,7 @@ struct XGeo {
   static constexpr int TARGET = F32 ? (XV == 0 ? 16 : (XV == 1 ? 8 : SLES_X_T2)) : (XV == 2 ? 8 : WARPS);
   static constexpr int MINB0 = TARGET / WARPS;
   static constexpr int MINB = MINB0 < 1 ? 1 : (MINB0 > 16 ? 16 : MINB0);
-  static constexpr size_t BASE = ((size_t)DIM * TE + SCR + N) * sizeof(C);  // + linear twiddle table
+  static constexpr size_t BASE = ((size_t)DIM * TE + SCR + F::LIN_LEN) * sizeof(C);  // + linear twiddle table
   // shared memory per block that keeps MINB blocks resident (228 KB per SM, 1 KB reserved per block)
   static constexpr size_t BUDGET = (228 / MINB - 1) * 1024;
 #ifndef SLES_X_NB
@@ -296,7 +296,7 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
   C* rst = reinterpret_cast<C*>(smem_raw);  // [D][N][W] projected components
   C* sm0 = rst + D * K::TE;                 // exchange scratch
   C* twt = sm0 + K::SCR;                    // twiddle table exp(-2 pi i e/N)
-  C* ring = twt + N;                        // NB tile buffers [N][W]
+  C* ring = twt + F::LIN_LEN;               // NB tile buffers [N][W]
   const StageCoef<Tp> SC = stage_coef<Tp>(A);
   const int tid = threadIdx.x;
   const int l = tid % W, j = tid / W;

@@ -3,8 +3,9 @@
 The loop, its CFL rule (dt = min(CFL dx/u_max, 0.1 dx^2/nu), with CFL = 0.3 on
 the first step), the NaN stop and the "time per gridpoint per timestep" print
 follow the reference.  Energy-spectrum snapshots go to Ek_plot_data.csv with
-the reference's binning; the PNG plot and the HDF5 field dumps are not
-produced (plotting and parallel HDF5 are outside this library).
+the reference's binning; field dumps (every ``file_out_time``) go to
+dumpfile/ as raw float64 files with XDMF descriptions instead of HDF5 (h5py
+is not used); the PNG plot is not produced (plotting is outside this library).
 """
 from __future__ import annotations
 
@@ -17,8 +18,9 @@ from . import ETD2_method as ETD2
 from . import RK3_method as RK3
 from . import RK4_method as RK4
 from .diagnostics import max_velocity, reference_binned_spectrum
+from .utilites import write_fields_xdmf
 
-__all__ = ["spectralMethodSolver", "find_max_velocity", "compute_dt"]
+__all__ = ["spectralMethodSolver", "find_max_velocity", "compute_dt", "output_h5"]
 
 
 def find_max_velocity(U, comm=None):
@@ -40,6 +42,21 @@ def compute_dt(U, u_max, nu, comm=None, dx=1.0, CFL=0.5):
     return dt
 
 
+def output_h5(domain, t, file_out_time, directory="dumpfile"):
+    """Write the physical velocity (2D: u, v and the vorticity) at time t, as
+    src/SM_solver.py:280-302 does, into ``directory``/dump{t//file_out_time}:
+    raw float64 files with an XDMF description (utilites.write_fields_xdmf;
+    h5py is not used)."""
+    d = domain
+    U = d.U.to("cpu").double().numpy()
+    if d.dim == 2:
+        fields = {"u": U[0], "v": U[1], "omega": d.curl.to("cpu").double().numpy()}
+    else:
+        fields = {"u": U[0], "v": U[1], "w": U[2]}
+    os.makedirs(directory, exist_ok=True)
+    return write_fields_xdmf(os.path.join(directory, f"dump{t // file_out_time:g}"), fields, d.dx, time=t)
+
+
 def _step(domain):
     if domain.method == "RK4":
         RK4.solveForNextTimestep(domain)
@@ -59,7 +76,7 @@ def spectralMethodSolver(domain, file_out_time: float = 0.0, No_Ek_plot: int = 5
     steps; the host synchronises once per chunk and at each E(k) snapshot,
     giving the same steps, dt sequence and snapshots as the host loop."""
     if device_dt:
-        return _solver_device_dt(domain, No_Ek_plot, verbose, chunk)
+        return _solver_device_dt(domain, file_out_time, No_Ek_plot, verbose, chunk)
     d = domain
     u_max = max_velocity(d)
     d.dt = compute_dt(None, u_max, d.nu, dx=d.dx, CFL=0.3)
@@ -70,7 +87,11 @@ def spectralMethodSolver(domain, file_out_time: float = 0.0, No_Ek_plot: int = 5
     d.U_hat1[...] = d.U_hat            # src/SM_solver.py:33
     columns = {}
     counter = 0
+    file_time = 0.0
     while True:
+        if file_out_time > 0 and t >= file_time:     # src/SM_solver.py:40-42
+            output_h5(d, t, file_out_time)
+            file_time += file_out_time
         if Ek_interval > 0 and t >= Ek_counter:
             tk, tE = reference_binned_spectrum(d)
             columns[f"k-{t:g}"] = tk
@@ -98,7 +119,7 @@ def spectralMethodSolver(domain, file_out_time: float = 0.0, No_Ek_plot: int = 5
     return counter
 
 
-def _solver_device_dt(d, No_Ek_plot, verbose, chunk):
+def _solver_device_dt(d, file_out_time, No_Ek_plot, verbose, chunk):
     import torch
 
     from . import _native as nat
@@ -110,14 +131,27 @@ def _solver_device_dt(d, No_Ek_plot, verbose, chunk):
     d.U_hat1[...] = d.U_hat            # src/SM_solver.py:33
     columns = {}
     Ek_counter = 0.0
-    if Ek_interval > 0:                # the first iteration's snapshot (t = dt_0 >= 0), taken here so
-        tk, tE = reference_binned_spectrum(d)  # that the first device step is never a paused one
-        t0 = compute_dt(None, max_velocity(d), d.nu, dx=d.dx, CFL=0.3)
-        columns[f"k-{t0:g}"] = tk
-        columns[f"Ek-{t0:g}"] = tE
-        Ek_counter += Ek_interval
-    c.ek_next = Ek_counter if Ek_interval > 0 else float("inf")
-    c.resumed = 1 if Ek_interval > 0 else 0
+    file_time = 0.0
+    inf = float("inf")
+
+    def events(t):
+        """The loop's per-iteration outputs (src/SM_solver.py:40-45) due at t."""
+        nonlocal Ek_counter, file_time
+        if file_out_time > 0 and t >= file_time:
+            output_h5(d, t, file_out_time)
+            file_time += file_out_time
+        if Ek_interval > 0 and t >= Ek_counter:
+            tk, tE = reference_binned_spectrum(d)
+            columns[f"k-{t:g}"] = tk
+            columns[f"Ek-{t:g}"] = tE
+            Ek_counter += Ek_interval
+        # the controller pauses when t reaches the earlier of the next two
+        return min(Ek_counter if Ek_interval > 0 else inf, file_time if file_out_time > 0 else inf)
+
+    # the first iteration's outputs (t = dt_0 >= 0) are written here, so that
+    # the first device step is never a paused one
+    c.ek_next = events(compute_dt(None, max_velocity(d), d.nu, dx=d.dx, CFL=0.3))
+    c.resumed = 1 if c.ek_next < inf else 0
     ctl = torch.frombuffer(bytearray(bytes(c)), dtype=torch.uint8).to(d.device)
     d._dtctl, d._parity = ctl, 0
     stepper = CapturedStepper(d)
@@ -133,11 +167,8 @@ def _solver_device_dt(d, No_Ek_plot, verbose, chunk):
             n_next = max(2, min(chunk, est))
             n_next += n_next % 2
             if st.flags & nat.DT_SNAPSHOT:
-                tk, tE = reference_binned_spectrum(d)
-                columns[f"k-{st.t:g}"] = tk
-                columns[f"Ek-{st.t:g}"] = tE
-                Ek_counter += Ek_interval
-                st.ek_next, st.flags, st.paused, st.resumed = Ek_counter, st.flags & ~nat.DT_SNAPSHOT, 0, 1
+                st.ek_next = events(st.t)
+                st.flags, st.paused, st.resumed = st.flags & ~nat.DT_SNAPSHOT, 0, 1
                 ctl.copy_(torch.frombuffer(bytearray(bytes(st)), dtype=torch.uint8))
                 continue
             if st.flags & nat.DT_NAN:

@@ -45,3 +45,22 @@ def test_device_dt_loop_matches_host_loop(case, tmp_path, monkeypatch):
     hb = (tmp_path / "dev" / "Ek_plot_data.csv").read_text().splitlines()
     assert ha[0] == hb[0] or case[1] == "float32"   # snapshot times in the column names
     assert len(ha) == len(hb)
+
+
+def test_field_dumps_match_between_loops(tmp_path, monkeypatch):
+    """file_out_time: the same dumps (names and contents) from both loops."""
+    import numpy as np
+    case = (32, "float64", "Smagorinsky", "RK3", True, 0.3)
+    for sub, dev in (("host", False), ("dev", True)):
+        (tmp_path / sub).mkdir()
+        monkeypatch.chdir(tmp_path / sub)
+        d = _dom(*case)
+        spectralMethodSolver(d, file_out_time=0.1, No_Ek_plot=2, verbose=False, device_dt=dev, chunk=4)
+    names = sorted(p.name for p in (tmp_path / "host" / "dumpfile").iterdir())
+    assert names == sorted(p.name for p in (tmp_path / "dev" / "dumpfile").iterdir())
+    assert len([n for n in names if n.endswith(".xdmf")]) >= 3
+    for n in names:
+        if n.endswith(".raw"):
+            a = np.fromfile(tmp_path / "host" / "dumpfile" / n)
+            b = np.fromfile(tmp_path / "dev" / "dumpfile" / n)
+            assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(a)
