@@ -248,7 +248,13 @@ struct EngineImpl final : Engine {
 #endif
   using FY = typename std::conditional<SLES_Y_PLANFOR != 0, typename PlanFor<Tp, N>::F, typename PlanLo<Tp, N>::F>::type;
   static constexpr int TZ = PlanFor<Tp, N / 2>::F::T;
-  static constexpr int LPI = cmax(1, 16 / TZ);
+#ifndef SLES_Z_LPI
+#define SLES_Z_LPI 0
+#endif
+  // z lines per work item: 8 threads' worth of lines (one line of 8 or more
+  // threads); at 256^3 one line per item ran the z pass 13% faster than two,
+  // at 128^3 7%, at 64^3 two and four were equal.  SLES_Z_LPI > 0 overrides.
+  static constexpr int LPI = SLES_Z_LPI > 0 ? SLES_Z_LPI : cmax(1, 8 / TZ);
 
   static C* slot(const PlanInfo& p, int i) {
     return reinterpret_cast<C*>(reinterpret_cast<char*>(p.ws) + slots_offset(DIM, N)) + (long long)i * p.hc_elems;
@@ -571,7 +577,8 @@ struct EngineImpl final : Engine {
   static constexpr int ADJ_FIELDS = 18;
   // lines per AZ work item: halved (keeping whole warps) when the staging
   // buffers and 24 line regions would not fit in shared memory
-  static constexpr int ALPI = (AZGeo<Tp, N, LPI>::SMEM > 227 * 1024 && LPI > 1) ? LPI / 2 : LPI;
+  static constexpr int LPI_ADJ = cmax(1, 16 / TZ);  // the adjoint's z lines per item (whole warps)
+  static constexpr int ALPI = (AZGeo<Tp, N, LPI_ADJ>::SMEM > 227 * 1024 && LPI_ADJ > 1) ? LPI_ADJ / 2 : LPI_ADJ;
   int adjoint_fields() const override { return DIM == 3 ? ADJ_FIELDS : 0; }
 
   AXArgs<Tp> axbase(const PlanInfo& pa) const {
