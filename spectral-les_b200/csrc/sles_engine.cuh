@@ -577,7 +577,13 @@ struct EngineImpl final : Engine {
   static constexpr int ADJ_FIELDS = 18;
   // lines per AZ work item: halved (keeping whole warps) when the staging
   // buffers and 24 line regions would not fit in shared memory
-  static constexpr int LPI_ADJ = cmax(1, 16 / TZ);  // the adjoint's z lines per item (whole warps)
+#ifndef SLES_AZ_LPI
+#define SLES_AZ_LPI 0
+#endif
+  // the adjoint's z lines per item: 8 threads' worth as the forward's (12
+  // groups x 8 threads keep whole warps; at 128^3 one line per item made the
+  // backward 7% faster than two).  SLES_AZ_LPI > 0 overrides.
+  static constexpr int LPI_ADJ = SLES_AZ_LPI > 0 ? SLES_AZ_LPI : cmax(1, 8 / TZ);
   static constexpr int ALPI = (AZGeo<Tp, N, LPI_ADJ>::SMEM > 227 * 1024 && LPI_ADJ > 1) ? LPI_ADJ / 2 : LPI_ADJ;
   int adjoint_fields() const override { return DIM == 3 ? ADJ_FIELDS : 0; }
 
