@@ -349,6 +349,25 @@ def cpu_oracle_rate(n, steps, warmup, seed, workers):
     return n ** 3 * steps / dt / 1e6, dt
 
 
+def max_over_ranks_of(x, world, device):
+    """The maximum of a per-rank float over all ranks of the default process group."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(points_per_rank, steps, secs_local, world, device):
+    """Whole-job Mpts*steps/s of ``world`` replicas (each rank advances its own
+    member of ``points_per_rank`` points): all ranks' points over the slowest
+    rank's time.  Returns (value, max seconds)."""
+    secs = max_over_ranks_of(secs_local, world, device)
+    return world * points_per_rank * steps / secs / 1e6, secs
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -568,11 +587,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(x, world, "cuda")
 
     n = args.n
     npts = float(n) ** 3
@@ -595,8 +610,7 @@ def main():
         secs = time_steps(d, args.steps, step)
     launches = _stepper.LAUNCHES[0]
     d._plan.check()  # no bounded wait gave up during the timed steps
-    secs = max_over_ranks(secs)
-    value = world * npts * args.steps / secs / 1e6
+    value, secs = replicas_value(npts, args.steps, secs, world, "cuda")
     ms_step = secs / args.steps * 1e3
 
     # per-kernel times (CUDA events, same stream) for the roofline
