@@ -381,6 +381,21 @@ def _nonlinear_projected(d, with_les):
     return N - P * d.K
 
 
+def _explicit_term(d, with_les):
+    """The explicit part of the corrected ETD2 scheme: P(mask N_hat [+ T_hat])
+    plus the linear forcing f U_hat on k != 0, added after the projection as
+    computeRHS adds it (src/RK4_method.py:58-64).  The reference's ETD2
+    forcing branch (src/ETD2_method.py:47-56) cannot run (it reads an unset
+    domain.epsilon); this follows the Cox-Matthews scheme with the forcing
+    treated explicitly."""
+    F = _nonlinear_projected(d, with_les)
+    if d.forcing > 0.0:
+        f = d.forcing * d.U_hat
+        f[(slice(None),) + (0,) * d.dim] = 0.0
+        F = F + f
+    return F
+
+
 def etd2_step(d):
     """src/ETD2_method.py:7-37.  Step 1 is RK4 (recording F1, parity) ; later
     steps advance with the exponential integrator."""
@@ -388,19 +403,18 @@ def etd2_step(d):
         if d.parity:
             rk4_step(d)
         else:
-            d.F1 = _nonlinear_projected(d, d.LES_ON)
-            if d.forcing > 0.0:
-                raise NotImplementedError("forcing with ETD2")
+            d.F1 = _explicit_term(d, d.LES_ON)
             d.method, m = "RK4", d.method
             rk4_step(d)
             d.method = m
         d.firstIteration = False
         return
-    if d.forcing > 0.0:
+    if d.forcing > 0.0 and d.parity:
         # src/ETD2_method.py:47-50 reads domain.epsilon, which is never set
         raise AttributeError("'InitializeDomain' object has no attribute 'epsilon'")
     d.F0 = d.F1
-    d.F1 = _nonlinear_projected(d, with_les=(d.LES_ON and not d.parity))
+    # parity: the reference evaluates u x omega only here (src/ETD2_method.py:39-46)
+    d.F1 = _nonlinear_projected(d, with_les=False) if d.parity else _explicit_term(d, d.LES_ON)
     E, c1, c0 = etd2_coefficients(d.K2, d.nu, d.dt, d.parity)
     if d.parity:
         d.U_hat = d.U_hat * E

@@ -64,9 +64,7 @@ def etd2_step(d):
     if d.firstIteration:
         if d.parity_mode:
             rk4_step(d, record_f1=True)
-        else:
-            if d.forcing > 0.0:
-                raise NotImplementedError("forcing with the corrected ETD2 scheme")
+        else:  # corrected: F1 = the explicit term (projected u x omega [+ stress] [+ forcing])
             uphys, cphys = d._phys_override()
             tmp = d._new_hc(d.dim)
             d._plan.rhs(d._s_uhat, tmp, d._s_f1, uphys, cphys)
@@ -74,8 +72,9 @@ def etd2_step(d):
             rk4_step(d)
         d.firstIteration = False
         return
-    if d.forcing > 0:
-        # src/ETD2_method.py:47-50 reads domain.epsilon, which the reference never sets
+    if d.forcing > 0 and d.parity_mode:
+        # src/ETD2_method.py:47-50 reads domain.epsilon, which the reference never sets;
+        # the corrected scheme treats the forcing explicitly (in F1)
         raise AttributeError("'InitializeDomain' object has no attribute 'epsilon'")
     U = d._s_uhat
     stage(d, 0, d.dt, U, None, d._s_f1, U, d._s_f0, 0, first=True)
