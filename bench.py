@@ -398,7 +398,7 @@ def bench_adjoint(rank):
     with a central difference in Cs (eps=1e-3, FP64)."""
     import torch
     from sles import RK4_method
-    from sles.adjoint import RK4Rollout, log_spectrum_misfit, shell_spectrum
+    from sles.adjoint import RK3Rollout, RK4Rollout, log_spectrum_misfit, shell_spectrum
     n, nu, dt, steps, cs = 128, 2e-4, 2e-3, 100, CS
     dT = make_domain(256, "float64", rank, method="RK4", les=None, nu=nu, dt=dt)
     dT.U_hat1[...] = dT.U_hat
@@ -431,6 +431,15 @@ def bench_adjoint(rank):
         res[name] = dict(fwd_ms=min(fw), bwd_ms=min(bw), loss=float(loss.detach()), g=g[..., : ro.nk].to(torch.complex128),
                          cs=float(c[0]), ro=ro, U=U)
     r32, r64 = res["f32"], res["f64"]
+    # the reference's RK3 with its adjoint, same recipe in FP32
+    ro3 = RK3Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=torch.float32, checkpoint_every=10)
+    U3 = U0.to(ro3.cdtype)
+    UT3 = ro3.forward_states(U3, cs, steps)[0][..., : ro3.nk].clone().requires_grad_(True)
+    gUT3, = torch.autograd.grad(log_spectrum_misfit(UT3, Et, n), [UT3])
+    ro3.timed(U3, cs, steps, gUT3)
+    t3 = [ro3.timed(U3, cs, steps, gUT3)[:2] for _ in range(3)]
+    f3, b3 = min(t[0] for t in t3), min(t[1] for t in t3)
+    del ro3, U3, UT3, gUT3
     # central difference in Cs on the FP64 path
     ro, U = r64["ro"], r64["U"]
     lo = lambda c: float(log_spectrum_misfit(ro.forward_states(U, c, steps)[0][..., : ro.nk], Et, n))
@@ -446,6 +455,8 @@ def bench_adjoint(rank):
            "dL_dCs_richardson_f64": fd, "cs_rel_err_f64_vs_richardson": abs(r64["cs"] - fd) / abs(fd),
            "cs_rel_err_f32_vs_richardson": abs(r32["cs"] - fd) / abs(fd),
            "grad_u0_rel_l2_f32_vs_f64": rel_l2(g32, g64),
+           "rk3": {"fwd_ms": round(f3, 2), "bwd_ms": round(b3, 2), "adjoint_fwd_ratio": round(b3 / f3, 3),
+                   "scheme": "the reference's RK3 (3 stages), FP32, same recipe"},
            "config": "128^3, random-phase spectrum k0=4, nu=2e-4, Smagorinsky Cs=0.17, RK4, dt=2e-3, 100 steps, "
                      "checkpoints every 10, loss on log E(k), k=1..43; backward = segment recompute + reverse stages"}
     del res, r32, r64, ro, U

@@ -234,6 +234,13 @@ int sles_rhs_static_workspace(sles_plan* plan, const void* u_hat, const void* u_
  *                       step), NULL to skip preparing it.  cs_grad (device
  *                       double, LES plans) accumulates dL/dCs.
  * All three field arguments hold 3 half-complex fields of the plan's layout.
+ *
+ * Plans of the reference's RK3 (scheme SLES_RK3, parity = 1; src/RK3_method.py:20-41,
+ * stages U_1 = U_0 + dt/2 k_0, U_2 = U_0 + dt k_1, output U_0 + dt k_2) use the
+ * same calls with stage = 2, 1, 0: seed lam = dt ubar; g = J(U_s)^T lam;
+ * acc += g; lam <- dt g (s=2), dt/2 g (s=1); at s=0 ubar <- acc and
+ * lam <- dt acc.  Other schemes (corrected SSP-RK3, ETD2) return
+ * SLES_ERR_UNSUPPORTED.
  */
 size_t sles_adjoint_workspace_bytes(const sles_plan* plan);
 int sles_adjoint_seed(sles_plan* plan, void* adj_ws, double dt, const void* ubar, void* acc, void* lam,

@@ -643,10 +643,37 @@ struct EngineImpl final : Engine {
     return launch_persistent(k_ypass<Tp, N, FY, 1, 0, 1>, items, K::THREADS, K::SMEM, st, a);
   }
 
+  // Reverse-stage coefficients of the plan's scheme.  The step output is
+  // U_0 + dt sum_s b_s k_s and stage s > 0 evaluates the RHS at U_0 + dt c_s k_{s-1}:
+  //   RK4 (src/RK4_method.py:20-35): b = (1/6, 1/3, 1/3, 1/6), c = (-, 1/2, 1/2, 1)
+  //   the reference's RK3 (src/RK3_method.py:20-41, parity = 1): the stages
+  //   U_0 + dt/2 k_0, U_0 - dt k_1 + 2 dt k_1 and the output U_0 + dt (k_2/6 + 2 k_2/3 + k_2/6)
+  //   give b = (0, 0, 1), c = (-, 1/2, 1).
+  // The corrected SSP-RK3 and ETD2 mix earlier stages into later ones and are not covered.
+  struct AdjScheme {
+    int ns;
+    double b[4], c[4];
+  };
+  static int adj_scheme(const PlanInfo& pa, AdjScheme* o) {
+    if (pa.d.scheme == SLES_RK4) {
+      *o = AdjScheme{4, {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0}, {0.0, 0.5, 0.5, 1.0}};
+      return SLES_OK;
+    }
+    if (pa.d.scheme == SLES_RK3 && pa.d.parity) {
+      *o = AdjScheme{3, {0.0, 0.0, 1.0 / 6.0 + 2.0 / 3.0 + 1.0 / 6.0, 0.0}, {0.0, 0.5, 1.0, 0.0}};
+      return SLES_OK;
+    }
+    return SLES_ERR_UNSUPPORTED;
+  }
   int adjoint_seed(PlanInfo& pa, double dt, const void* ubar, void* acc, void* lam, cudaStream_t st) override {
-    if (DIM != 3) return SLES_ERR_UNSUPPORTED;
-    return launch(k_adj_seed<Tp>, 1184, 256, 0, st, (const C*)ubar, (C*)acc, (C*)lam, 3 * pa.hc_elems,
-                  (Tp)(dt / 6.0));
+    if constexpr (DIM != 3) {
+      return SLES_ERR_UNSUPPORTED;
+    } else {
+      AdjScheme sc;
+      SLES_TRY(adj_scheme(pa, &sc));
+      return launch(k_adj_seed<Tp>, 1184, 256, 0, st, (const C*)ubar, (C*)acc, (C*)lam, 3 * pa.hc_elems,
+                    (Tp)(sc.b[sc.ns - 1] * dt));
+    }
   }
   int adjoint_prime(PlanInfo& pa, const void* u_state, const void* lam, cudaStream_t st) override {
     if constexpr (DIM != 3) {
@@ -667,7 +694,9 @@ struct EngineImpl final : Engine {
       return SLES_ERR_UNSUPPORTED;
     } else {
       if (pa.ws_fields < ADJ_FIELDS) return SLES_ERR_WORKSPACE;
-      if (s < 0 || s > 3) return SLES_ERR_INVALID_ARG;
+      AdjScheme sc;
+      SLES_TRY(adj_scheme(pa, &sc));
+      if (s < 0 || s >= sc.ns) return SLES_ERR_INVALID_ARG;
       SLES_TRY(aypass(pa, 1, st));
       switch (pa.d.les_model) {
         case SLES_LES_SMAGORINSKY: SLES_TRY(azpass<M_SMAG>(pa, csgrad, st)); break;
@@ -682,11 +711,9 @@ struct EngineImpl final : Engine {
       a.ubar = (C*)ubar;
       a.acc = (C*)acc;
       a.lam = (C*)lam;
-      // reverse RK4 stage s: lam <- alpha ubar + beta g;  s = 0: ubar <- acc, lam <- dt/6 acc
-      static const double al[4] = {1.0 / 6.0, 1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0};
-      static const double be[4] = {0.0, 0.5, 0.5, 1.0};
-      a.alpha = (Tp)(al[s] * dt);
-      a.beta = (Tp)(be[s] * dt);
+      // reverse stage s: lam <- b_{s-1} dt ubar + c_s dt g;  s = 0: ubar <- acc, lam <- b_last dt acc
+      a.alpha = (Tp)((s > 0 ? sc.b[s - 1] : sc.b[sc.ns - 1]) * dt);
+      a.beta = (Tp)(sc.c[s] * dt);
       a.last = (s == 0) ? 1 : 0;
       return axpass(pa, a, st);
     }

@@ -1,5 +1,5 @@
-"""Differentiable RK4 rollouts: the fused forward steps with a hand-written
-discrete adjoint behind ``torch.autograd.Function`` (3D).
+"""Differentiable RK4 and RK3 rollouts: the fused forward steps with a
+hand-written discrete adjoint behind ``torch.autograd.Function`` (3D).
 
     ro = RK4Rollout(n=128, nu=2e-4, dt=2e-3, les="Smagorinsky", dtype=torch.float32,
                     checkpoint_every=10)
@@ -13,9 +13,13 @@ The forward keeps the state every ``checkpoint_every`` steps.  The backward
 walks the segments from the last to the first: it recomputes a segment's
 steps from its checkpoint, keeping each step's four stage states, then runs
 the reverse stages (``sles_adjoint_stage``, the transpose of the fused
-right-hand side and of the RK4 combination) through it.  Gradients follow
-torch's convention for complex tensors (dL/dRe + i dL/dIm of every stored
-half-complex entry), so they compare directly with torch.fft autograd.
+right-hand side and of the step's stage combination) through it.  Gradients
+follow torch's convention for complex tensors (dL/dRe + i dL/dIm of every
+stored half-complex entry), so they compare directly with torch.fft autograd.
+
+``RK3Rollout`` is the same for the reference's RK3 (src/RK3_method.py:20-41,
+whose stages are U_0 + dt/2 k_0, U_0 + dt k_1 and the output U_0 + dt k_2).
+The corrected SSP-RK3 and ETD2 have no adjoint here.
 """
 from __future__ import annotations
 
@@ -26,14 +30,18 @@ import torch
 from . import _native as nat
 from . import autotune
 
-__all__ = ["RK4Rollout", "shell_spectrum", "log_spectrum_misfit"]
+__all__ = ["RK4Rollout", "RK3Rollout", "shell_spectrum", "log_spectrum_misfit"]
 
 _SIZES = (16, 24, 32, 48, 64, 96, 128, 256, 512)
 
 
 class RK4Rollout:
+    METHOD = "RK4"
+
     def __init__(self, n, nu, dt, les="Smagorinsky", Cs=0.17, dtype=torch.float32, parity=True, forcing=0.0,
                  checkpoint_every=10, device="cuda"):
+        if self.METHOD == "RK3" and not parity:
+            raise ValueError("the adjoint covers the reference's RK3 only (parity=True)")
         if int(n) not in _SIZES:
             raise ValueError("grid N=%d is not compiled (supported: %s)" % (n, _SIZES))
         if checkpoint_every < 1:
@@ -50,8 +58,10 @@ class RK4Rollout:
         self.rdtype = dtype
         self.cdtype = torch.complex64 if dtype == torch.float32 else torch.complex128
         self.device = torch.device(device)
-        self.plan = nat.Plan(3, self.n, dtype, model, nat.SCHEME_RK4, parity, nu, Cs, forcing, self.device)
-        autotune.apply_cached(self.plan, "RK4")
+        scheme = nat.SCHEME_RK4 if self.METHOD == "RK4" else nat.SCHEME_RK3
+        self.ns = 4 if self.METHOD == "RK4" else 3  # stages per step
+        self.plan = nat.Plan(3, self.n, dtype, model, scheme, parity, nu, Cs, forcing, self.device)
+        autotune.apply_cached(self.plan, self.METHOD)
         self.nk, self.nkp = self.plan.nk, self.plan.nkp
         self._ws_owner, self._ws = self.plan.adjoint_workspace()
         self._store = []   # stage states of the segment being reversed (reused across calls)
@@ -73,23 +83,29 @@ class RK4Rollout:
         return s[..., : self.nk].clone()
 
     # ---- forward ----
+    def _flags(self, rk, primed):
+        f = nat.STAGE_PRIMED if (primed and rk == 0) or rk > 0 else 0
+        return f | (nat.STAGE_RK4 if self.ns == 4 else 0)
+
     def _step(self, A, B, Cacc, primed):
-        """One fused RK4 step from A (kept) into B; Cacc is the accumulator
+        """One fused step from A (kept) into B; Cacc is the RK4 accumulator
         (overwritten).  Returns True (the workspace is primed with B)."""
-        Cacc.copy_(A)  # U_hat1 = U_hat at step entry (SM_solver.py:33)
-        for rk in range(4):
-            flags = nat.STAGE_RK4 | (nat.STAGE_PRIMED if (primed and rk == 0) or rk > 0 else 0)
-            self.plan.stage(rk, self.dt, A if rk == 0 else B, A, Cacc, B, None, None, None, flags)
+        if self.ns == 4:
+            Cacc.copy_(A)  # U_hat1 = U_hat at step entry (SM_solver.py:33)
+        for rk in range(self.ns):
+            self.plan.stage(rk, self.dt, A if rk == 0 else B, A, Cacc if self.ns == 4 else None, B, None, None,
+                            None, self._flags(rk, primed))
         return True
 
     def _step_keep(self, A, stages, Cacc, primed):
-        """As _step, writing the stage states U_1..U_3 to stages[0..2] and the
-        step output to stages[3]."""
-        Cacc.copy_(A)
+        """As _step, writing the stage states U_1..U_{ns-1} to stages[0..ns-2]
+        and the step output to stages[ns-1]."""
+        if self.ns == 4:
+            Cacc.copy_(A)
         cur = A
-        for rk in range(4):
-            flags = nat.STAGE_RK4 | (nat.STAGE_PRIMED if (primed and rk == 0) or rk > 0 else 0)
-            self.plan.stage(rk, self.dt, cur, A, Cacc, stages[rk], None, None, None, flags)
+        for rk in range(self.ns):
+            self.plan.stage(rk, self.dt, cur, A, Cacc if self.ns == 4 else None, stages[rk], None, None, None,
+                            self._flags(rk, primed))
             cur = stages[rk]
         return True
 
@@ -119,7 +135,8 @@ class RK4Rollout:
         Cacc = self._new()
         store = self._store
         while len(store) < max(e - s for s, e in zip(starts, ends)):
-            store.append([self._new() for _ in range(4)])
+            store.append([self._new() for _ in range(self.ns)])
+        last = self.ns - 1
         for s0, s1 in reversed(list(zip(starts, ends))):
             m = s1 - s0
             # recompute the segment: inputs[i] = state entering step s0 + i
@@ -127,16 +144,16 @@ class RK4Rollout:
             primed = False
             for i in range(m):
                 primed = self._step_keep(inputs[i], store[i], Cacc, primed)
-                inputs.append(store[i][3])
-            # stage states of step i: U_0 = inputs[i], U_1..U_3 = store[i][0..2]
+                inputs.append(store[i][last])
+            # stage states of step i: U_0 = inputs[i], U_1..U_last = store[i][0..last-1]
             states = lambda i, s: inputs[i] if s == 0 else store[i][s - 1]
-            self.plan.adjoint_prime(self._ws, states(m - 1, 3), lam)
+            self.plan.adjoint_prime(self._ws, states(m - 1, last), lam)
             for i in range(m - 1, -1, -1):
-                for s in (3, 2, 1, 0):
+                for s in range(last, -1, -1):
                     if s > 0:
                         un = states(i, s - 1)
                     else:
-                        un = states(i - 1, 3) if i > 0 else None
+                        un = states(i - 1, last) if i > 0 else None
                     self.plan.adjoint_stage(self._ws, s, dt, un, ubar, acc, lam, csg)
         return ubar, csg
 
@@ -158,6 +175,12 @@ class RK4Rollout:
         e[2].record(st)
         torch.cuda.synchronize(self.device)
         return e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), UT, g, c
+
+
+class RK3Rollout(RK4Rollout):
+    """The reference's RK3 (src/RK3_method.py:20-41, parity arithmetic) with its
+    discrete adjoint; same arguments and use as ``RK4Rollout``."""
+    METHOD = "RK3"
 
 
 class _RolloutFn(torch.autograd.Function):

@@ -1,9 +1,10 @@
-"""The hand-written discrete adjoint of the fused RK4 rollout.
+"""The hand-written discrete adjoint of the fused RK4 and reference-RK3 rollouts.
 
 Checked three ways: against torch.fft autograd through the plain torch path
 (float64, same arithmetic up to rounding), against central finite differences
 of the fused forward (float64), and float32 against float64 at the adjoint
-configuration's full size (128^3, 100 steps, checkpoints every 10).
+configuration's full size (128^3, 100 steps, checkpoints every 10).  Schemes
+without an adjoint (corrected SSP-RK3, ETD2) are refused through the C ABI.
 """
 import math
 
@@ -11,7 +12,8 @@ import numpy as np
 import pytest
 import torch
 
-from sles.adjoint import RK4Rollout, log_spectrum_misfit, shell_spectrum
+from sles import _native as nat
+from sles.adjoint import RK3Rollout, RK4Rollout, log_spectrum_misfit, shell_spectrum
 from sles.plain_torch import PlainSolver
 from sles.synthetic import random_spectrum_velocity
 
@@ -27,11 +29,17 @@ def _rel(a, b):
     return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
 
 
+_ROLLOUT = {"RK4": RK4Rollout, "RK3": RK3Rollout}
+_UNSUPPORTED = 2  # SLES_ERR_UNSUPPORTED, include/sles.h
+
+
+@pytest.mark.parametrize("method", ["RK4", "RK3"])
 @pytest.mark.parametrize("les", ["Smagorinsky", "vreman", None])
-def test_one_step_vjp_matches_torch_autograd(les):
+def test_one_step_vjp_matches_torch_autograd(les, method):
     n, nu, dt, cs = 32, 3e-3, 5e-3, 0.17
-    ro = RK4Rollout(n, nu, dt, les=les, Cs=cs, dtype=torch.float64, checkpoint_every=1)
-    ps = PlainSolver(n, 3, nu=nu, dt=dt, les=les, Cs=cs, method="RK4", device="cuda")
+    ro = _ROLLOUT[method](n, nu, dt, les=les, Cs=cs, dtype=torch.float64, checkpoint_every=1)
+    ps = PlainSolver(n, 3, nu=nu, dt=dt, les=les, Cs=cs, method=method, device="cuda")
+    step = ps.rk4 if method == "RK4" else ps.rk3
     U0 = ps.rfft(_field(n))
     g = torch.Generator(device="cuda").manual_seed(1)
     lam = torch.complex(torch.randn(U0.shape, generator=g, device="cuda", dtype=torch.float64),
@@ -39,14 +47,14 @@ def test_one_step_vjp_matches_torch_autograd(les):
     # torch autograd through the plain path
     Ua = U0.clone().requires_grad_(True)
     Ca = torch.tensor(cs, dtype=torch.float64, device="cuda", requires_grad=True)
-    La = (torch.conj(lam) * ps.rk4(Ua, Ca)).real.sum()
+    La = (torch.conj(lam) * step(Ua, Ca)).real.sum()
     gU_ref, = torch.autograd.grad(La, [Ua], retain_graph=True)
     gC_ref = torch.autograd.grad(La, [Ca])[0] if les else None
     # the fused path and its adjoint
     Ub = U0.clone().requires_grad_(True)
     Cb = torch.tensor(cs, dtype=torch.float64, device="cuda", requires_grad=True)
     UT = ro(Ub, Cb, 1)
-    assert _rel(UT.detach(), ps.rk4(U0).detach()) < 1e-12
+    assert _rel(UT.detach(), step(U0).detach()) < 1e-12
     Lb = (torch.conj(lam) * UT).real.sum()
     Lb.backward()
     assert _rel(Ub.grad, gU_ref) < 1e-10
@@ -54,10 +62,11 @@ def test_one_step_vjp_matches_torch_autograd(les):
         assert abs(float(Cb.grad) - float(gC_ref)) <= 1e-9 * abs(float(gC_ref))
 
 
-def test_checkpointed_rollout_matches_torch_autograd():
+@pytest.mark.parametrize("method", ["RK4", "RK3"])
+def test_checkpointed_rollout_matches_torch_autograd(method):
     n, nu, dt, cs, steps = 32, 2e-3, 5e-3, 0.17, 7
-    ro = RK4Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=torch.float64, checkpoint_every=3)
-    ps = PlainSolver(n, 3, nu=nu, dt=dt, les="Smagorinsky", Cs=cs, method="RK4", device="cuda")
+    ro = _ROLLOUT[method](n, nu, dt, les="Smagorinsky", Cs=cs, dtype=torch.float64, checkpoint_every=3)
+    ps = PlainSolver(n, 3, nu=nu, dt=dt, les="Smagorinsky", Cs=cs, method=method, device="cuda")
     U0 = ps.rfft(_field(n, seed=4))
     Et = shell_spectrum(U0, n).detach() * 0.9
     Ua = U0.clone().requires_grad_(True)
@@ -79,10 +88,10 @@ def _loss(ro, U0, cs, steps, Et, n):
                                          Et, n))
 
 
-@pytest.mark.parametrize("les", ["Smagorinsky", "vreman"])
-def test_gradients_match_central_differences(les):
+@pytest.mark.parametrize("les,method", [("Smagorinsky", "RK4"), ("vreman", "RK4"), ("Smagorinsky", "RK3")])
+def test_gradients_match_central_differences(les, method):
     n, nu, dt, cs, steps = 48, 2e-4, 2e-3, 0.17, 12
-    ro = RK4Rollout(n, nu, dt, les=les, Cs=cs, dtype=torch.float64, checkpoint_every=5)
+    ro = _ROLLOUT[method](n, nu, dt, les=les, Cs=cs, dtype=torch.float64, checkpoint_every=5)
     U0 = ro.rfft(_field(n, seed=6))
     Et = shell_spectrum(U0, n).detach() * torch.linspace(0.8, 1.2, shell_spectrum(U0, n).numel(), device="cuda",
                                                          dtype=torch.float64)
@@ -124,3 +133,21 @@ def test_adjoint_configuration_float32_against_float64():
     (g64, c64), (g32, c32) = grads
     assert _rel(g32, g64) < 1e-3
     assert abs(c32 - c64) <= 1e-3 * abs(c64)
+
+
+@pytest.mark.parametrize("scheme,parity", [(nat.SCHEME_RK3, False), (nat.SCHEME_ETD2, False), (nat.SCHEME_ETD2, True)])
+def test_schemes_without_an_adjoint_are_refused(scheme, parity):
+    """The corrected SSP-RK3 and ETD2 mix earlier stages into later ones; the
+    adjoint entry points return SLES_ERR_UNSUPPORTED for their plans."""
+    n = 32
+    plan = nat.Plan(3, n, torch.float64, nat.LES_SMAGORINSKY, scheme, parity, 1e-3, 0.17, 0.0, torch.device("cuda"))
+    _, ws = plan.adjoint_workspace()
+    z = torch.zeros((3, n, n, plan.nkp), dtype=torch.complex128, device="cuda")
+    with pytest.raises(nat.SlesError) as e:
+        plan.adjoint_seed(ws, 1e-3, z, z.clone(), z.clone())
+    assert e.value.status == _UNSUPPORTED
+    csg = torch.zeros(1, dtype=torch.float64, device="cuda")
+    with pytest.raises(nat.SlesError) as e:
+        plan.adjoint_stage(ws, 0, 1e-3, None, z, z.clone(), z.clone(), csg)
+    assert e.value.status == _UNSUPPORTED
+    torch.cuda.synchronize()
