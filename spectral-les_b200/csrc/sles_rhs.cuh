@@ -243,7 +243,10 @@ struct XGeo {
 #ifndef SLES_X_W2
 #define SLES_X_W2 4
 #endif
-  static constexpr int W = (XV == 2) ? (F32 ? SLES_X_W2 : 2) : (F32 ? 8 : 4);
+#ifndef SLES_X_W0
+#define SLES_X_W0 8
+#endif
+  static constexpr int W = (XV == 2) ? (F32 ? SLES_X_W2 : 2) : (F32 ? (XV == 0 ? SLES_X_W0 : 8) : 4);
   static constexpr int T = F::T, V = F::V;
   static constexpr int THREADS = W * T;
   static constexpr int TE = N * W;
@@ -252,7 +255,10 @@ struct XGeo {
 #ifndef SLES_X_T2
 #define SLES_X_T2 12
 #endif
-  static constexpr int TARGET = F32 ? (XV == 0 ? 16 : (XV == 1 ? 8 : SLES_X_T2)) : (XV == 2 ? 8 : WARPS);
+#ifndef SLES_X_T0
+#define SLES_X_T0 16
+#endif
+  static constexpr int TARGET = F32 ? (XV == 0 ? SLES_X_T0 : (XV == 1 ? 8 : SLES_X_T2)) : (XV == 2 ? 8 : WARPS);
   static constexpr int MINB0 = TARGET / WARPS;
   static constexpr int MINB = MINB0 < 1 ? 1 : (MINB0 > 16 ? 16 : MINB0);
   static constexpr size_t BASE = ((size_t)DIM * TE + SCR + F::LIN_LEN) * sizeof(C);  // + linear twiddle table
