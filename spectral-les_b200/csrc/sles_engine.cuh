@@ -243,10 +243,19 @@ struct EngineImpl final : Engine {
   // per x-pass variant: the 32-byte-row tiles (XV 2) pad the exchange every 8 points
   template <int XV>
   using FXV = typename WithPad<typename PlanLo<Tp, N>::F, XV == 2 ? 8 : SLES_X_PADD>::F;
-#ifndef SLES_Y_PLANFOR
-#define SLES_Y_PLANFOR 0
+  // y-pass FFT plans per direction: PlanFor (more points per thread) or PlanLo.
+  // At N = 512 in FP32 the inverse pass (6 inputs) runs fastest on PlanFor
+  // (32 threads per line) and the forward pass (9 inputs) on PlanLo (64).
+#ifndef SLES_YI_PLANFOR
+#define SLES_YI_PLANFOR -1
 #endif
-  using FY = typename std::conditional<SLES_Y_PLANFOR != 0, typename PlanFor<Tp, N>::F, typename PlanLo<Tp, N>::F>::type;
+#ifndef SLES_YF_PLANFOR
+#define SLES_YF_PLANFOR 0
+#endif
+  static constexpr bool YI_FOR = SLES_YI_PLANFOR >= 0 ? SLES_YI_PLANFOR != 0 : (N == 512 && sizeof(Tp) == 4);
+  using FYI = typename std::conditional<YI_FOR, typename PlanFor<Tp, N>::F, typename PlanLo<Tp, N>::F>::type;
+  using FYF = typename std::conditional<SLES_YF_PLANFOR != 0, typename PlanFor<Tp, N>::F,
+                                        typename PlanLo<Tp, N>::F>::type;
   static constexpr int TZ = PlanFor<Tp, N / 2>::F::T;
 #ifndef SLES_Z_LPI
 #define SLES_Z_LPI 0
@@ -274,7 +283,8 @@ struct EngineImpl final : Engine {
     return (N == 128 || N == 256) ? 2 : 0;
   }
   static int ychunks(const PlanInfo& p) {                                 // y-pass column chunks
-    constexpr int WY = TGeo<Tp, N, FY>::W;
+    constexpr int WY = TGeo<Tp, N, FYI>::W;
+    static_assert(TGeo<Tp, N, FYF>::W == WY, "one tile width for both y directions");
     return (p.nk + WY - 1) / WY;
   }
 
@@ -364,7 +374,8 @@ struct EngineImpl final : Engine {
   template <int LES>
   int ypass(const PlanInfo& p, int inv, cudaStream_t st) {
     if (DIM != 3) return SLES_OK;
-    using K = TGeo<Tp, N, FY>;
+    using K = TGeo<Tp, N, FYI>;  // tile geometry (the tensor map) is the same for FYF
+    using KF = TGeo<Tp, N, FYF>;
     YArgs<Tp> a{};
     const long long cb = sizeof(C);
     SLES_TRY(make_tmap(&a.tm, slot(p, 0), K::EPC, p.nk, N, (long long)p.nkp * cb, N, (long long)N * p.nkp * cb,
@@ -376,8 +387,8 @@ struct EngineImpl final : Engine {
     a.nk = p.nk;
     a.nchunks = ychunks(p);
     const long long items = (long long)N * ychunks(p);
-    if (inv) return launch_persistent(k_ypass<Tp, N, FY, LES, 1>, items, K::THREADS, K::SMEM, st, a);
-    return launch_persistent(k_ypass<Tp, N, FY, LES, 0>, items, K::THREADS, K::SMEM, st, a);
+    if (inv) return launch_persistent(k_ypass<Tp, N, FYI, LES, 1>, items, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_ypass<Tp, N, FYF, LES, 0>, items, KF::THREADS, KF::SMEM, st, a);
   }
 
   template <int LES, int MODEL, int PAR2D>
@@ -627,7 +638,8 @@ struct EngineImpl final : Engine {
                              a);
   }
   int aypass(const PlanInfo& pa, int inv, cudaStream_t st) {
-    using K = TGeo<Tp, N, FY>;
+    using K = TGeo<Tp, N, FYI>;
+    using KF = TGeo<Tp, N, FYF>;
     YArgs<Tp> a{};
     const long long cb = sizeof(C);
     SLES_TRY(make_tmap(&a.tm, slot(pa, 0), K::EPC, pa.nk, N, (long long)pa.nkp * cb, N, (long long)N * pa.nkp * cb,
@@ -639,8 +651,8 @@ struct EngineImpl final : Engine {
     a.nk = pa.nk;
     a.nchunks = ychunks(pa);
     const long long items = (long long)N * ychunks(pa);
-    if (inv) return launch_persistent(k_ypass<Tp, N, FY, 1, 1, 1>, items, K::THREADS, K::SMEM, st, a);
-    return launch_persistent(k_ypass<Tp, N, FY, 1, 0, 1>, items, K::THREADS, K::SMEM, st, a);
+    if (inv) return launch_persistent(k_ypass<Tp, N, FYI, 1, 1, 1>, items, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_ypass<Tp, N, FYF, 1, 0, 1>, items, KF::THREADS, KF::SMEM, st, a);
   }
 
   // Reverse-stage coefficients of the plan's scheme.  The step output is

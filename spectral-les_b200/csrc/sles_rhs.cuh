@@ -200,12 +200,15 @@ template <typename Tp, int N, class F, bool RING = true, int NBUF_SET = 0>
 struct TGeo {
   using C = typename CT<Tp>::C;
 #ifndef SLES_Y_W
-#define SLES_Y_W 8
+#define SLES_Y_W 0
 #endif
 #ifndef SLES_Y_NBUF
 #define SLES_Y_NBUF 0
 #endif
-  static constexpr int W = (sizeof(Tp) == 4) ? SLES_Y_W : 4;  // 64-byte tile rows
+  // FP32: 64-byte tile rows, 128-byte rows at N = 512 (at 512^3, with the
+  // 32-thread inverse line plan, the y passes took 1.75 + 2.01 ms against
+  // 2.21 + 2.06; at 256^3 the wider rows were slower); FP64: 64-byte rows
+  static constexpr int W = (sizeof(Tp) == 4) ? (SLES_Y_W > 0 ? SLES_Y_W : (N == 512 ? 16 : 8)) : 4;
   static constexpr int EPC = sizeof(C) / 8;                 // 8-byte tensor elements per complex
   static constexpr int T = F::T, V = F::V;
   static constexpr int THREADS = W * T;
