@@ -244,18 +244,25 @@ struct EngineImpl final : Engine {
   template <int XV>
   using FXV = typename WithPad<typename PlanLo<Tp, N>::F, XV == 2 ? 8 : SLES_X_PADD>::F;
   // y-pass FFT plans per direction: PlanFor (more points per thread) or PlanLo.
-  // At N = 512 in FP32 the inverse pass (6 inputs) runs fastest on PlanFor
-  // (32 threads per line) and the forward pass (9 inputs) on PlanLo (64).
+  // At N = 512 in FP32 the LES inverse pass (6 inputs, 128-byte rows) runs
+  // fastest on PlanFor (32 threads per line), the LES forward pass (9 inputs)
+  // and the passes without LES on PlanLo (64).
 #ifndef SLES_YI_PLANFOR
 #define SLES_YI_PLANFOR -1
 #endif
 #ifndef SLES_YF_PLANFOR
 #define SLES_YF_PLANFOR 0
 #endif
-  static constexpr bool YI_FOR = SLES_YI_PLANFOR >= 0 ? SLES_YI_PLANFOR != 0 : (N == 512 && sizeof(Tp) == 4);
-  using FYI = typename std::conditional<YI_FOR, typename PlanFor<Tp, N>::F, typename PlanLo<Tp, N>::F>::type;
+  template <int LES>
+  using FYI = typename std::conditional<(SLES_YI_PLANFOR >= 0 ? SLES_YI_PLANFOR != 0
+                                                              : (N == 512 && sizeof(Tp) == 4 && LES != 0)),
+                                        typename PlanFor<Tp, N>::F, typename PlanLo<Tp, N>::F>::type;
   using FYF = typename std::conditional<SLES_YF_PLANFOR != 0, typename PlanFor<Tp, N>::F,
                                         typename PlanLo<Tp, N>::F>::type;
+  template <int LES>
+  using YGeoI = TGeo<Tp, N, FYI<LES>, true, 0, LES>;
+  template <int LES>
+  using YGeoF = TGeo<Tp, N, FYF, true, 0, LES>;
   static constexpr int TZ = PlanFor<Tp, N / 2>::F::T;
 #ifndef SLES_Z_LPI
 #define SLES_Z_LPI 0
@@ -282,9 +289,10 @@ struct EngineImpl final : Engine {
     if (N <= 64) return 1;
     return (N == 128 || N == 256) ? 2 : 0;
   }
+  template <int LES>
   static int ychunks(const PlanInfo& p) {                                 // y-pass column chunks
-    constexpr int WY = TGeo<Tp, N, FYI>::W;
-    static_assert(TGeo<Tp, N, FYF>::W == WY, "one tile width for both y directions");
+    constexpr int WY = YGeoI<LES>::W;
+    static_assert(YGeoF<LES>::W == WY, "one tile width for both y directions");
     return (p.nk + WY - 1) / WY;
   }
 
@@ -374,8 +382,8 @@ struct EngineImpl final : Engine {
   template <int LES>
   int ypass(const PlanInfo& p, int inv, cudaStream_t st) {
     if (DIM != 3) return SLES_OK;
-    using K = TGeo<Tp, N, FYI>;  // tile geometry (the tensor map) is the same for FYF
-    using KF = TGeo<Tp, N, FYF>;
+    using K = YGeoI<LES>;  // tile geometry (the tensor map) is the same for the forward plan
+    using KF = YGeoF<LES>;
     YArgs<Tp> a{};
     const long long cb = sizeof(C);
     SLES_TRY(make_tmap(&a.tm, slot(p, 0), K::EPC, p.nk, N, (long long)p.nkp * cb, N, (long long)N * p.nkp * cb,
@@ -385,9 +393,9 @@ struct EngineImpl final : Engine {
     a.fs = p.hc_elems;
     a.nkp = p.nkp;
     a.nk = p.nk;
-    a.nchunks = ychunks(p);
-    const long long items = (long long)N * ychunks(p);
-    if (inv) return launch_persistent(k_ypass<Tp, N, FYI, LES, 1>, items, K::THREADS, K::SMEM, st, a);
+    a.nchunks = ychunks<LES>(p);
+    const long long items = (long long)N * ychunks<LES>(p);
+    if (inv) return launch_persistent(k_ypass<Tp, N, FYI<LES>, LES, 1>, items, K::THREADS, K::SMEM, st, a);
     return launch_persistent(k_ypass<Tp, N, FYF, LES, 0>, items, KF::THREADS, KF::SMEM, st, a);
   }
 
@@ -638,8 +646,8 @@ struct EngineImpl final : Engine {
                              a);
   }
   int aypass(const PlanInfo& pa, int inv, cudaStream_t st) {
-    using K = TGeo<Tp, N, FYI>;
-    using KF = TGeo<Tp, N, FYF>;
+    using K = YGeoI<1>;
+    using KF = YGeoF<1>;
     YArgs<Tp> a{};
     const long long cb = sizeof(C);
     SLES_TRY(make_tmap(&a.tm, slot(pa, 0), K::EPC, pa.nk, N, (long long)pa.nkp * cb, N, (long long)N * pa.nkp * cb,
@@ -649,9 +657,9 @@ struct EngineImpl final : Engine {
     a.fs = pa.hc_elems;
     a.nkp = pa.nkp;
     a.nk = pa.nk;
-    a.nchunks = ychunks(pa);
-    const long long items = (long long)N * ychunks(pa);
-    if (inv) return launch_persistent(k_ypass<Tp, N, FYI, 1, 1, 1>, items, K::THREADS, K::SMEM, st, a);
+    a.nchunks = ychunks<1>(pa);
+    const long long items = (long long)N * ychunks<1>(pa);
+    if (inv) return launch_persistent(k_ypass<Tp, N, FYI<1>, 1, 1, 1>, items, K::THREADS, K::SMEM, st, a);
     return launch_persistent(k_ypass<Tp, N, FYF, 1, 0, 1>, items, KF::THREADS, KF::SMEM, st, a);
   }
 

@@ -196,7 +196,7 @@ __device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& 
 // Strided-axis pass geometry: one work item (W lines of N points) per block
 // iteration; tiles arrive by TMA into a ring of NBUF buffers.
 // ---------------------------------------------------------------------------
-template <typename Tp, int N, class F, bool RING = true, int NBUF_SET = 0>
+template <typename Tp, int N, class F, bool RING = true, int NBUF_SET = 0, int WIDE = 0>
 struct TGeo {
   using C = typename CT<Tp>::C;
 #ifndef SLES_Y_W
@@ -205,10 +205,12 @@ struct TGeo {
 #ifndef SLES_Y_NBUF
 #define SLES_Y_NBUF 0
 #endif
-  // FP32: 64-byte tile rows, 128-byte rows at N = 512 (at 512^3, with the
-  // 32-thread inverse line plan, the y passes took 1.75 + 2.01 ms against
-  // 2.21 + 2.06; at 256^3 the wider rows were slower); FP64: 64-byte rows
-  static constexpr int W = (sizeof(Tp) == 4) ? (SLES_Y_W > 0 ? SLES_Y_W : (N == 512 ? 16 : 8)) : 4;
+  // FP32: 64-byte tile rows; WIDE (the LES passes) at N = 512: 128-byte rows
+  // (at 512^3, with the 32-thread inverse line plan, the LES y passes took
+  // 1.75 + 2.01 ms against 2.21 + 2.06; the passes without LES and all passes
+  // at 256^3 were slower with the wider rows); FP64: 64-byte rows
+  static constexpr int W =
+      (sizeof(Tp) == 4) ? (SLES_Y_W > 0 ? SLES_Y_W : ((N == 512 && WIDE) ? 16 : 8)) : 4;
   static constexpr int EPC = sizeof(C) / 8;                 // 8-byte tensor elements per complex
   static constexpr int T = F::T, V = F::V;
   static constexpr int THREADS = W * T;
@@ -517,9 +519,9 @@ struct YArgs {
 // groups (the recomputed state and the cotangent), the forward contracts
 // Z_j - i ky A2_j.
 template <typename Tp, int N, class F, int LES, int INV, int ADJ = 0>
-__global__ void __launch_bounds__(TGeo<Tp, N, F>::THREADS, TGeo<Tp, N, F>::MINB)
+__global__ void __launch_bounds__(TGeo<Tp, N, F, true, 0, LES>::THREADS, TGeo<Tp, N, F, true, 0, LES>::MINB)
 k_ypass(const __grid_constant__ YArgs<Tp> A) {
-  using K = TGeo<Tp, N, F>;
+  using K = TGeo<Tp, N, F, true, 0, LES>;
   using C = typename CT<Tp>::C;
   constexpr int T = K::T, V = K::V, W = K::W;
   constexpr int KIND = ADJ ? (INV ? 6 : 7) : (INV ? (LES ? 0 : 1) : (LES ? 2 : 3));
