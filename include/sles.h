@@ -239,8 +239,13 @@ int sles_rhs_static_workspace(sles_plan* plan, const void* u_hat, const void* u_
  * stages U_1 = U_0 + dt/2 k_0, U_2 = U_0 + dt k_1, output U_0 + dt k_2) use the
  * same calls with stage = 2, 1, 0: seed lam = dt ubar; g = J(U_s)^T lam;
  * acc += g; lam <- dt g (s=2), dt/2 g (s=1); at s=0 ubar <- acc and
- * lam <- dt acc.  Other schemes (corrected SSP-RK3, ETD2) return
- * SLES_ERR_UNSUPPORTED.
+ * lam <- dt acc.  Plans of the corrected SSP-RK3 (SLES_RK3, parity = 0;
+ * U_1 = U_0 + dt k_0, U_2 = 3/4 U_0 + 1/4 (U_1 + dt k_1), output
+ * 1/3 U_0 + 2/3 (U_2 + dt k_2)) run the reverse stages in Shu-Osher form:
+ * seed acc = ubar/3, lam = 2/3 dt ubar; s=2: w = 2/3 ubar + g, acc += 3/4 w,
+ * ubar <- w/4, lam <- dt/4 w; s=1: w = ubar + g, acc += w, lam <- dt w;
+ * s=0: w = acc + g, ubar <- w (the gradient w.r.t. the step input),
+ * acc <- w/3, lam <- 2/3 dt w.  ETD2 plans return SLES_ERR_UNSUPPORTED.
  */
 size_t sles_adjoint_workspace_bytes(const sles_plan* plan);
 int sles_adjoint_seed(sles_plan* plan, void* adj_ws, double dt, const void* ubar, void* acc, void* lam,

@@ -39,6 +39,14 @@
 //   s = 3: lam <- dt/3 ubar + dt g;   s = 2: lam <- dt/3 ubar + dt/2 g
 //   s = 1: lam <- dt/6 ubar + dt/2 g; s = 0: ubar <- acc, lam <- dt/6 acc (next step back)
 // Seed: acc = ubar, lam = dt/6 ubar.
+//
+// The corrected SSP-RK3 (U_1 = U_0 + dt k_0, U_2 = 3/4 U_0 + 1/4 (U_1 + dt k_1),
+// output 1/3 U_0 + 2/3 (U_2 + dt k_2)) runs in Shu-Osher form, ubar carrying
+// the cotangent of the latest stage state:
+//   seed: acc = ubar/3, lam = 2/3 dt ubar
+//   s = 2: w = 2/3 ubar + g; acc += 3/4 w; ubar <- w/4; lam <- dt/4 w
+//   s = 1: w = ubar + g;     acc += w;                  lam <- dt w
+//   s = 0: w = acc + g;      ubar <- w (gradient of the step input); acc <- w/3; lam <- 2/3 dt w
 #pragma once
 #include "sles_rhs.cuh"
 
@@ -59,6 +67,10 @@ struct AXArgs {
   C* lam;
   Tp alpha, beta;      // lam <- alpha ubar + beta g;  last: ubar <- acc, lam <- alpha acc
   int last;
+  // Shu-Osher form (SSP-RK3): w = pu ubar + g (last: w = acc + g); acc += pa w
+  // (last: acc <- pa w); ubar <- pb w (last: ubar <- w); lam <- pl w
+  int ssp;
+  Tp pu, pa, pb, pl;
   Tp nu, forcing;
   double kmax;
 };
@@ -152,13 +164,27 @@ k_adj_xpass(const __grid_constant__ AXArgs<Tp> A) {
             const C lc = A.lam[o];
             g = csub(g, cscale(lc, A.nu * (Tp)k2));
             if (A.forcing > (Tp)0 && k2 != 0) g = cadd(g, cscale(lc, A.forcing));
-            const C an = cadd(A.acc[o], g);
-            A.acc[o] = an;
-            if (A.last) {
-              A.ubar[o] = an;
-              ln = cscale(an, A.alpha);
+            if (A.ssp) {
+              if (A.last) {
+                const C w = cadd(A.acc[o], g);
+                A.ubar[o] = w;
+                A.acc[o] = cscale(w, A.pa);
+                ln = cscale(w, A.pl);
+              } else {
+                const C w = cadd(cscale(A.ubar[o], A.pu), g);
+                A.acc[o] = cadd(A.acc[o], cscale(w, A.pa));
+                A.ubar[o] = cscale(w, A.pb);
+                ln = cscale(w, A.pl);
+              }
             } else {
-              ln = cadd(cscale(A.ubar[o], A.alpha), cscale(g, A.beta));
+              const C an = cadd(A.acc[o], g);
+              A.acc[o] = an;
+              if (A.last) {
+                A.ubar[o] = an;
+                ln = cscale(an, A.alpha);
+              } else {
+                ln = cadd(cscale(A.ubar[o], A.alpha), cscale(g, A.beta));
+              }
             }
             A.lam[o] = ln;
           }
@@ -459,13 +485,13 @@ k_adj_zpass(const AZArgs<Tp> A) {
   }
 }
 
-// acc = ubar, lam = alpha ubar over n complex elements (adjoint seed)
+// acc = sacc ubar, lam = alpha ubar over n complex elements (adjoint seed)
 template <typename Tp>
 __global__ void k_adj_seed(const typename CT<Tp>::C* __restrict__ ubar, typename CT<Tp>::C* __restrict__ acc,
-                           typename CT<Tp>::C* __restrict__ lam, long long n, Tp alpha) {
+                           typename CT<Tp>::C* __restrict__ lam, long long n, Tp alpha, Tp sacc) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const auto v = ubar[i];
-    acc[i] = v;
+    acc[i] = cscale(v, sacc);
     lam[i] = cscale(v, alpha);
   }
 }

@@ -18,8 +18,9 @@ follow torch's convention for complex tensors (dL/dRe + i dL/dIm of every
 stored half-complex entry), so they compare directly with torch.fft autograd.
 
 ``RK3Rollout`` is the same for the reference's RK3 (src/RK3_method.py:20-41,
-whose stages are U_0 + dt/2 k_0, U_0 + dt k_1 and the output U_0 + dt k_2).
-The corrected SSP-RK3 and ETD2 have no adjoint here.
+whose stages are U_0 + dt/2 k_0, U_0 + dt k_1 and the output U_0 + dt k_2)
+or, with ``parity=False``, for the corrected SSP-RK3 (Shu & Osher 1988).
+ETD2 has no adjoint here.
 """
 from __future__ import annotations
 
@@ -40,8 +41,6 @@ class RK4Rollout:
 
     def __init__(self, n, nu, dt, les="Smagorinsky", Cs=0.17, dtype=torch.float32, parity=True, forcing=0.0,
                  checkpoint_every=10, device="cuda"):
-        if self.METHOD == "RK3" and not parity:
-            raise ValueError("the adjoint covers the reference's RK3 only (parity=True)")
         if int(n) not in _SIZES:
             raise ValueError("grid N=%d is not compiled (supported: %s)" % (n, _SIZES))
         if checkpoint_every < 1:
@@ -178,8 +177,9 @@ class RK4Rollout:
 
 
 class RK3Rollout(RK4Rollout):
-    """The reference's RK3 (src/RK3_method.py:20-41, parity arithmetic) with its
-    discrete adjoint; same arguments and use as ``RK4Rollout``."""
+    """The reference's RK3 (src/RK3_method.py:20-41, ``parity=True``) or the
+    corrected SSP-RK3 (``parity=False``) with its discrete adjoint; same
+    arguments and use as ``RK4Rollout``."""
     METHOD = "RK3"
 
 
