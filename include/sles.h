@@ -245,7 +245,15 @@ int sles_rhs_static_workspace(sles_plan* plan, const void* u_hat, const void* u_
  * seed acc = ubar/3, lam = 2/3 dt ubar; s=2: w = 2/3 ubar + g, acc += 3/4 w,
  * ubar <- w/4, lam <- dt/4 w; s=1: w = ubar + g, acc += w, lam <- dt w;
  * s=0: w = acc + g, ubar <- w (the gradient w.r.t. the step input),
- * acc <- w/3, lam <- 2/3 dt w.  ETD2 plans return SLES_ERR_UNSUPPORTED.
+ * acc <- w/3, lam <- 2/3 dt w.  Plans of the corrected ETD2 (SLES_ETD2,
+ * parity = 0; U_{n+1} = E U_n + w1 F(U_n) + w0 F(U_{n-1}), F without the
+ * viscous term, weights at z = dt nu k^2 as in sles_stage) take one reverse
+ * step per call: seed lam = w1 ubar (acc unused); stage 0: g = J_F(U_n)^T lam,
+ * w = E ubar + g, lam <- w1 w + w0 ubar, ubar <- w; stage 1 (the step after
+ * the first, RK4, step): the same with lam <- w0 ubar, the cotangent of
+ * F(U_0); stage 2: ubar <- ubar + J_F(u_state)^T lam (applied after the RK4
+ * step's reverse on an RK4 plan).  The reference's ETD2 (parity = 1) returns
+ * SLES_ERR_UNSUPPORTED.
  */
 size_t sles_adjoint_workspace_bytes(const sles_plan* plan);
 int sles_adjoint_seed(sles_plan* plan, void* adj_ws, double dt, const void* ubar, void* acc, void* lam,

@@ -73,7 +73,27 @@ struct AXArgs {
   Tp pu, pa, pb, pl;
   Tp nu, forcing;
   double kmax;
+  // corrected ETD2 (F excludes the viscous term, which E carries):
+  // 1: w = E ubar + g; lam <- w1 w + w0 ubar; ubar <- w
+  // 2: the step after the first (RK4) step: as 1 with lam <- w0 ubar (the
+  //    cotangent of F(U_0), applied by mode 3 after the RK4 step's reverse)
+  // 3: ubar <- ubar + g
+  int etd;
+  double dt_d, nu_d;
 };
+
+// Cox & Matthews (2002) ETD2 weights at z = dt nu k^2 (the forward's
+// corrected branch, update_component in sles_rhs.cuh)
+__device__ __forceinline__ void etd2_weights(double h, double z, double& E, double& w1, double& w0) {
+  E = exp(-z);
+  if (fabs(z) < 1e-2) {
+    w1 = h * (1.5 - 2.0 * z / 3.0 + z * z / 4.0 - z * z * z / 15.0);
+    w0 = h * (-0.5 + z / 6.0 - z * z / 24.0 + z * z * z / 120.0);
+  } else {
+    w1 = h * ((1.0 - z) * E - 1.0 + 2.0 * z) / (z * z);
+    w0 = h * (-E + 1.0 - z) / (z * z);
+  }
+}
 
 // m = h * mask * P(lam) at one mode (in place on s[3])
 template <typename Tp>
@@ -162,9 +182,21 @@ k_adj_xpass(const __grid_constant__ AXArgs<Tp> A) {
             const int kx = kx_at(m);
             const int k2 = kx * kx + kyv * kyv + col * col;
             const C lc = A.lam[o];
-            g = csub(g, cscale(lc, A.nu * (Tp)k2));
+            if (!A.etd) g = csub(g, cscale(lc, A.nu * (Tp)k2));
             if (A.forcing > (Tp)0 && k2 != 0) g = cadd(g, cscale(lc, A.forcing));
-            if (A.ssp) {
+            if (A.etd) {
+              const C ub = A.ubar[o];
+              if (A.etd == 3) {
+                A.ubar[o] = cadd(ub, g);
+                ln = lc;
+              } else {
+                double E, w1, w0;
+                etd2_weights(A.dt_d, A.dt_d * A.nu_d * (double)k2, E, w1, w0);
+                const C w = cadd(cscale(ub, (Tp)E), g);
+                A.ubar[o] = w;
+                ln = (A.etd == 1) ? cadd(cscale(w, (Tp)w1), cscale(ub, (Tp)w0)) : cscale(ub, (Tp)w0);
+              }
+            } else if (A.ssp) {
               if (A.last) {
                 const C w = cadd(A.acc[o], g);
                 A.ubar[o] = w;
@@ -482,6 +514,29 @@ k_adj_zpass(const AZArgs<Tp> A) {
       for (int w = 0; w < (K::THREADS + 31) / 32; ++w) s += red[w];
       atomicAdd(A.csgrad, s * A.csfac);
     }
+  }
+}
+
+// lam = w1(k) ubar on every stored mode of the 3 half-complex fields (the
+// corrected ETD2 seed; w1 the step's F_n weight at z = dt nu k^2)
+template <typename Tp>
+__global__ void k_adj_seed_etd(const typename CT<Tp>::C* __restrict__ ubar, typename CT<Tp>::C* __restrict__ lam,
+                               long long fs, int n, int nkp, int nk, double dt, double nu) {
+  const long long tot = 3LL * fs;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
+    const long long e = i % fs;
+    const int kz = (int)(e % nkp);
+    const long long r = e / nkp;
+    const int y = (int)(r % n);
+    const long long x = r / n;
+    if (kz >= nk || x >= n) {
+      lam[i] = cmk<typename CT<Tp>::C>(0, 0);
+      continue;
+    }
+    const int kx = kc2c((int)x, n), ky = kc2c(y, n);
+    double E, w1, w0;
+    etd2_weights(dt, dt * nu * (double)(kx * kx + ky * ky + kz * kz), E, w1, w0);
+    lam[i] = cscale(ubar[i], (Tp)w1);
   }
 }
 

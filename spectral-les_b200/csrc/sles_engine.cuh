@@ -669,23 +669,30 @@ struct EngineImpl final : Engine {
   //   the reference's RK3 (src/RK3_method.py:20-41, parity = 1): the stages
   //   U_0 + dt/2 k_0, U_0 - dt k_1 + 2 dt k_1 and the output U_0 + dt (k_2/6 + 2 k_2/3 + k_2/6)
   //   give b = (0, 0, 1), c = (-, 1/2, 1).
-  // The corrected SSP-RK3 (parity = 0) runs in Shu-Osher form (ssp = 1, see
-  // sles_adjoint.cuh); ETD2 carries F0 across steps and is not covered.
+  // The corrected SSP-RK3 (parity = 0) runs in Shu-Osher form (ssp = 1) and
+  // the corrected ETD2 in its two-step form (etd = 1; stage 0: a reverse
+  // step, 1: the step after the first RK4 step, 2: the cotangent of F(U_0)),
+  // see sles_adjoint.cuh.  The reference's ETD2 (parity = 1) is not covered.
   struct AdjScheme {
     int ns, ssp;
     double b[4], c[4];
+    int etd;
   };
   static int adj_scheme(const PlanInfo& pa, AdjScheme* o) {
     if (pa.d.scheme == SLES_RK4) {
-      *o = AdjScheme{4, 0, {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0}, {0.0, 0.5, 0.5, 1.0}};
+      *o = AdjScheme{4, 0, {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0}, {0.0, 0.5, 0.5, 1.0}, 0};
       return SLES_OK;
     }
     if (pa.d.scheme == SLES_RK3 && pa.d.parity) {
-      *o = AdjScheme{3, 0, {0.0, 0.0, 1.0 / 6.0 + 2.0 / 3.0 + 1.0 / 6.0, 0.0}, {0.0, 0.5, 1.0, 0.0}};
+      *o = AdjScheme{3, 0, {0.0, 0.0, 1.0 / 6.0 + 2.0 / 3.0 + 1.0 / 6.0, 0.0}, {0.0, 0.5, 1.0, 0.0}, 0};
       return SLES_OK;
     }
     if (pa.d.scheme == SLES_RK3) {  // SSP-RK3, Shu & Osher (1988)
-      *o = AdjScheme{3, 1, {0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+      *o = AdjScheme{3, 1, {0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}, 0};
+      return SLES_OK;
+    }
+    if (pa.d.scheme == SLES_ETD2 && !pa.d.parity) {  // Cox & Matthews (2002)
+      *o = AdjScheme{3, 0, {0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}, 1};
       return SLES_OK;
     }
     return SLES_ERR_UNSUPPORTED;
@@ -696,6 +703,9 @@ struct EngineImpl final : Engine {
     } else {
       AdjScheme sc;
       SLES_TRY(adj_scheme(pa, &sc));
+      if (sc.etd)  // lam = w1(k) ubar
+        return launch(k_adj_seed_etd<Tp>, 1184, 256, 0, st, (const C*)ubar, (C*)lam, pa.hc_elems, N, pa.nkp, pa.nk,
+                      dt, pa.d.nu);
       if (sc.ssp)  // acc = ubar/3, lam = 2/3 dt ubar
         return launch(k_adj_seed<Tp>, 1184, 256, 0, st, (const C*)ubar, (C*)acc, (C*)lam, 3 * pa.hc_elems,
                       (Tp)(2.0 / 3.0 * dt), (Tp)(1.0 / 3.0));
@@ -744,6 +754,9 @@ struct EngineImpl final : Engine {
       a.beta = (Tp)(sc.c[s] * dt);
       a.last = (s == 0) ? 1 : 0;
       a.ssp = sc.ssp;
+      a.etd = sc.etd ? s + 1 : 0;
+      a.dt_d = dt;
+      a.nu_d = pa.d.nu;
       if (sc.ssp) {  // Shu-Osher reverse stages of SSP-RK3 (sles_adjoint.cuh)
         static const double pu[3] = {0.0, 1.0, 2.0 / 3.0}, pa3[3] = {1.0 / 3.0, 1.0, 0.75},
                             pb[3] = {1.0, 1.0, 0.25}, pl[3] = {2.0 / 3.0, 1.0, 0.25};

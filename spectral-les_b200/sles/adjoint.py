@@ -20,7 +20,9 @@ stored half-complex entry), so they compare directly with torch.fft autograd.
 ``RK3Rollout`` is the same for the reference's RK3 (src/RK3_method.py:20-41,
 whose stages are U_0 + dt/2 k_0, U_0 + dt k_1 and the output U_0 + dt k_2)
 or, with ``parity=False``, for the corrected SSP-RK3 (Shu & Osher 1988).
-ETD2 has no adjoint here.
+``ETD2Rollout`` is the corrected ETD2 (Cox & Matthews 2002) with the
+reference's step structure (src/ETD2_method.py:7-57: the first step records
+F(U_0) and runs RK4); the reference's own ETD2 weights have no adjoint.
 """
 from __future__ import annotations
 
@@ -31,7 +33,7 @@ import torch
 from . import _native as nat
 from . import autotune
 
-__all__ = ["RK4Rollout", "RK3Rollout", "shell_spectrum", "log_spectrum_misfit"]
+__all__ = ["RK4Rollout", "RK3Rollout", "ETD2Rollout", "shell_spectrum", "log_spectrum_misfit"]
 
 _SIZES = (16, 24, 32, 48, 64, 96, 128, 256, 512)
 
@@ -181,6 +183,77 @@ class RK3Rollout(RK4Rollout):
     corrected SSP-RK3 (``parity=False``) with its discrete adjoint; same
     arguments and use as ``RK4Rollout``."""
     METHOD = "RK3"
+
+
+class ETD2Rollout:
+    """Corrected ETD2 with its discrete adjoint (3D).  The first step records
+    F(U_0) and runs RK4 (src/ETD2_method.py:7-14); later steps are
+    U_{n+1} = E U_n + w1 F(U_n) + w0 F(U_{n-1}) with E = exp(-dt nu k^2) and
+    F the explicit term (projected u x omega, LES stress, forcing).  The
+    forward keeps every step's input state for the reverse sweep, which runs
+    the ETD2 reverse steps on this plan and the first step's RK4 reverse on a
+    companion RK4 plan.  Same call and gradient conventions as ``RK4Rollout``.
+    """
+
+    def __init__(self, n, nu, dt, les="Smagorinsky", Cs=0.17, dtype=torch.float32, forcing=0.0, device="cuda"):
+        self.rk = RK4Rollout(n, nu, dt, les=les, Cs=Cs, dtype=dtype, forcing=forcing, checkpoint_every=1,
+                             device=device)
+        self.n, self.nu, self.dt, self.forcing = self.rk.n, self.rk.nu, self.rk.dt, self.rk.forcing
+        self.rdtype, self.cdtype, self.device = self.rk.rdtype, self.rk.cdtype, self.rk.device
+        self.plan = nat.Plan(3, self.n, dtype, self.rk.les, nat.SCHEME_ETD2, False, nu, Cs, forcing, self.device)
+        autotune.apply_cached(self.plan, "ETD2")
+        self.nk, self.nkp = self.plan.nk, self.plan.nkp
+        self._ws_owner, self._ws = self.plan.adjoint_workspace()
+        self.rfft = self.rk.rfft
+
+    def _new(self):
+        return self.rk._new()
+
+    def forward_states(self, U0, Cs, nsteps):
+        """Run ``nsteps`` steps; return (U_T padded, [U_0 .. U_{T-1}] padded)."""
+        nsteps = int(nsteps)
+        if nsteps < 1:
+            raise ValueError("nsteps must be >= 1")
+        for p in (self.plan, self.rk.plan):
+            p.set_params(self.nu, Cs, self.forcing)
+        A = self.rk._pad(U0)
+        states = [A]
+        F1, tmp = self._new(), self._new()
+        self.plan.rhs(A, tmp, F1)  # F(U_0), src/ETD2_method.py:8-14
+        U, Cacc = self._new(), self._new()
+        self.rk._step(A, U, Cacc, False)  # first step: RK4
+        F0 = tmp
+        for k in range(1, nsteps):
+            states.append(U.clone())
+            # U <- E U + w1 F(U) + w0 F1; F0 <- F(U) (src/ETD2_method.py:16-37)
+            self.plan.stage(0, self.dt, U, None, F1, U, F0, None, None, nat.STAGE_PRIMED if k > 1 else 0)
+            F0, F1 = F1, F0
+        return U, states
+
+    def backward_states(self, states, gUT, Cs, nsteps):
+        """Reverse sweep; returns (dL/dU_0 padded, dL/dCs float64 tensor)."""
+        nsteps = int(nsteps)
+        self.plan.set_params(self.nu, Cs, self.forcing)
+        csg = torch.zeros(1, dtype=torch.float64, device=self.device)
+        ubar = self.rk._pad(gUT)
+        if nsteps > 1:
+            lam, acc = self._new(), self._new()
+            self.plan.adjoint_seed(self._ws, self.dt, ubar, acc, lam)  # lam = w1 ubar
+            self.plan.adjoint_prime(self._ws, states[nsteps - 1], lam)
+            for k in range(nsteps - 1, 0, -1):
+                # stage 0: a reverse ETD2 step; 1: the step after the RK4 step, which
+                # leaves lam = the cotangent of F(U_0) and primes at U_0
+                self.plan.adjoint_stage(self._ws, 0 if k > 1 else 1, self.dt, states[k - 1], ubar, acc, lam, csg)
+        # the RK4 step's reverse from dL/dU_1
+        g, c = self.rk.backward_states({0: states[0]}, ubar[..., : self.nk], Cs, 1)
+        if nsteps > 1:  # + J_F(U_0)^T (cotangent of F(U_0))
+            self.plan.adjoint_stage(self._ws, 2, self.dt, None, g, acc, lam, csg)
+        return g, csg + c
+
+    def __call__(self, U0, Cs, nsteps):
+        if not torch.is_tensor(Cs):
+            Cs = torch.tensor(float(Cs), dtype=torch.float64, device=self.device)
+        return _RolloutFn.apply(U0, Cs, self, int(nsteps))
 
 
 class _RolloutFn(torch.autograd.Function):

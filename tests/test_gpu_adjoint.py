@@ -4,8 +4,9 @@ Checked three ways: against torch.fft autograd through the plain torch path
 (float64, same arithmetic up to rounding), against central finite differences
 of the fused forward (float64), and float32 against float64 at the adjoint
 configuration's full size (128^3, 100 steps, checkpoints every 10).  RK3 is
-the reference's scheme, SSP3 the corrected SSP-RK3 (parity=False).  ETD2,
-which has no adjoint, is refused through the C ABI.
+the reference's scheme, SSP3 the corrected SSP-RK3 (parity=False); ETD2 the
+corrected ETD2 (its first step RK4), whose reference-weight form has no
+adjoint and is refused through the C ABI.
 """
 import math
 
@@ -14,7 +15,7 @@ import pytest
 import torch
 
 from sles import _native as nat
-from sles.adjoint import RK3Rollout, RK4Rollout, log_spectrum_misfit, shell_spectrum
+from sles.adjoint import ETD2Rollout, RK3Rollout, RK4Rollout, log_spectrum_misfit, shell_spectrum
 from sles.plain_torch import PlainSolver
 from sles.synthetic import random_spectrum_velocity
 
@@ -145,10 +146,60 @@ def test_adjoint_configuration_float32_against_float64():
     assert abs(c32 - c64) <= 1e-3 * abs(c64)
 
 
-@pytest.mark.parametrize("scheme,parity", [(nat.SCHEME_ETD2, False), (nat.SCHEME_ETD2, True)])
+@pytest.mark.parametrize("steps", [1, 2, 4])
+@pytest.mark.parametrize("les", ["Smagorinsky", "vreman", None])
+def test_etd2_rollout_matches_torch_autograd(les, steps):
+    n, nu, dt, cs = 32, 3e-3, 5e-3, 0.17
+    ro = ETD2Rollout(n, nu, dt, les=les, Cs=cs, dtype=torch.float64)
+    ps = PlainSolver(n, 3, nu=nu, dt=dt, les=les, Cs=cs, method="ETD2", parity=False, device="cuda")
+    U0 = ps.rfft(_field(n, seed=8))
+    g = torch.Generator(device="cuda").manual_seed(2)
+    lam = torch.complex(torch.randn(U0.shape, generator=g, device="cuda", dtype=torch.float64),
+                        torch.randn(U0.shape, generator=g, device="cuda", dtype=torch.float64))
+    Ua = U0.clone().requires_grad_(True)
+    Ca = torch.tensor(cs, dtype=torch.float64, device="cuda", requires_grad=True)
+    ps.first = True
+    out = Ua
+    for _ in range(steps):
+        out = ps.step(out, Ca)
+    La = (torch.conj(lam) * out).real.sum()
+    gU_ref, = torch.autograd.grad(La, [Ua], retain_graph=True)
+    gC_ref = torch.autograd.grad(La, [Ca])[0] if les else None
+    Ub = U0.clone().requires_grad_(True)
+    Cb = torch.tensor(cs, dtype=torch.float64, device="cuda", requires_grad=True)
+    UT = ro(Ub, Cb, steps)
+    assert _rel(UT.detach(), out.detach()) < 1e-12
+    (torch.conj(lam) * UT).real.sum().backward()
+    assert _rel(Ub.grad, gU_ref) < 1e-10
+    if les:
+        assert abs(float(Cb.grad) - float(gC_ref)) <= 1e-9 * abs(float(gC_ref))
+
+
+def test_etd2_gradients_match_central_differences():
+    n, nu, dt, cs, steps = 48, 2e-4, 2e-3, 0.17, 12
+    ro = ETD2Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=torch.float64)
+    U0 = ro.rfft(_field(n, seed=6))
+    Et = shell_spectrum(U0, n).detach() * torch.linspace(0.8, 1.2, shell_spectrum(U0, n).numel(), device="cuda",
+                                                         dtype=torch.float64)
+    U = U0.clone().requires_grad_(True)
+    C = torch.tensor(cs, dtype=torch.float64, device="cuda", requires_grad=True)
+    log_spectrum_misfit(ro(U, C, steps), Et, n).backward()
+    cd = lambda e: (_loss(ro, U0, cs + e, steps, Et, n) - _loss(ro, U0, cs - e, steps, Et, n)) / (2 * e)
+    fd1, fd2 = cd(1e-3), cd(5e-4)
+    rich = (4.0 * fd2 - fd1) / 3.0
+    assert abs(rich - float(C.grad)) <= 1e-5 * abs(rich)
+    d = ro.rfft(_field(n, seed=123))
+    d = d / torch.linalg.vector_norm(d) * torch.linalg.vector_norm(U0)
+    h = 1e-5
+    fd = (_loss(ro, U0 + h * d, cs, steps, Et, n) - _loss(ro, U0 - h * d, cs, steps, Et, n)) / (2 * h)
+    an = float((torch.conj(U.grad) * d).real.sum())
+    assert abs(fd - an) <= 1e-5 * abs(fd)
+
+
+@pytest.mark.parametrize("scheme,parity", [(nat.SCHEME_ETD2, True)])
 def test_schemes_without_an_adjoint_are_refused(scheme, parity):
-    """ETD2 carries F0 from step to step; the adjoint entry points return
-    SLES_ERR_UNSUPPORTED for its plans."""
+    """The reference's ETD2 weights (parity arithmetic) have no adjoint; the
+    adjoint entry points return SLES_ERR_UNSUPPORTED for its plans."""
     n = 32
     plan = nat.Plan(3, n, torch.float64, nat.LES_SMAGORINSKY, scheme, parity, 1e-3, 0.17, 0.0, torch.device("cuda"))
     _, ws = plan.adjoint_workspace()
