@@ -116,7 +116,10 @@ __device__ __forceinline__ void adj_project(typename CT<Tp>::C (&s)[3], const in
 // ---------------------------------------------------------------------------
 // AX pass.  Work item = (ky slice, chunk of W kz columns); lines along x.
 // ---------------------------------------------------------------------------
-template <typename Tp, int N, class F>
+// MODE (compile time, so each scheme's kernel carries only its own update):
+// 0 the diagonal Runge-Kutta form (RK4, the reference's RK3), 1 Shu-Osher
+// (SSP-RK3), 2 corrected ETD2.
+template <typename Tp, int N, class F, int MODE>
 __global__ void __launch_bounds__(XGeo<Tp, N, F, 3, 0>::THREADS, XGeo<Tp, N, F, 3, 0>::MINB)
 k_adj_xpass(const __grid_constant__ AXArgs<Tp> A) {
   using K = XGeo<Tp, N, F, 3, 0>;
@@ -182,9 +185,9 @@ k_adj_xpass(const __grid_constant__ AXArgs<Tp> A) {
             const int kx = kx_at(m);
             const int k2 = kx * kx + kyv * kyv + col * col;
             const C lc = A.lam[o];
-            if (!A.etd) g = csub(g, cscale(lc, A.nu * (Tp)k2));
+            if constexpr (MODE != 2) g = csub(g, cscale(lc, A.nu * (Tp)k2));
             if (A.forcing > (Tp)0 && k2 != 0) g = cadd(g, cscale(lc, A.forcing));
-            if (A.etd) {
+            if constexpr (MODE == 2) {
               const C ub = A.ubar[o];
               if (A.etd == 3) {
                 A.ubar[o] = cadd(ub, g);
@@ -196,7 +199,7 @@ k_adj_xpass(const __grid_constant__ AXArgs<Tp> A) {
                 A.ubar[o] = w;
                 ln = (A.etd == 1) ? cadd(cscale(w, (Tp)w1), cscale(ub, (Tp)w0)) : cscale(ub, (Tp)w0);
               }
-            } else if (A.ssp) {
+            } else if constexpr (MODE == 1) {
               if (A.last) {
                 const C w = cadd(A.acc[o], g);
                 A.ubar[o] = w;

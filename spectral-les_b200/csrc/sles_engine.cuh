@@ -622,7 +622,9 @@ struct EngineImpl final : Engine {
   int axpass(const PlanInfo& pa, const AXArgs<Tp>& a, cudaStream_t st) {
     using K = XGeo<Tp, N, FX, 3, 0>;
     const long long items = (long long)N * xchunks<0>(pa);
-    return launch_persistent(k_adj_xpass<Tp, N, FX>, items, K::THREADS, K::SMEM, st, a);
+    if (a.etd) return launch_persistent(k_adj_xpass<Tp, N, FX, 2>, items, K::THREADS, K::SMEM, st, a);
+    if (a.ssp) return launch_persistent(k_adj_xpass<Tp, N, FX, 1>, items, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_adj_xpass<Tp, N, FX, 0>, items, K::THREADS, K::SMEM, st, a);
   }
   template <int MODEL>
   int azpass(const PlanInfo& pa, double* csgrad, cudaStream_t st) {
