@@ -398,7 +398,7 @@ def bench_adjoint(rank):
     with a central difference in Cs (eps=1e-3, FP64)."""
     import torch
     from sles import RK4_method
-    from sles.adjoint import RK3Rollout, RK4Rollout, log_spectrum_misfit, shell_spectrum
+    from sles.adjoint import ETD2Rollout, RK3Rollout, RK4Rollout, log_spectrum_misfit, shell_spectrum
     n, nu, dt, steps, cs = 128, 2e-4, 2e-3, 100, CS
     dT = make_domain(256, "float64", rank, method="RK4", les=None, nu=nu, dt=dt)
     dT.U_hat1[...] = dT.U_hat
@@ -440,6 +440,26 @@ def bench_adjoint(rank):
     t3 = [ro3.timed(U3, cs, steps, gUT3)[:2] for _ in range(3)]
     f3, b3 = min(t[0] for t in t3), min(t[1] for t in t3)
     del ro3, U3, UT3, gUT3
+    # the corrected ETD2 with its adjoint (every step's state kept), same recipe in FP32
+    roe = ETD2Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=torch.float32)
+    Ue = U0.to(roe.cdtype)
+    UTe = roe.forward_states(Ue, cs, steps)[0][..., : roe.nk].clone().requires_grad_(True)
+    gUTe, = torch.autograd.grad(log_spectrum_misfit(UTe, Et, n), [UTe])
+    st = torch.cuda.current_stream()
+    te = []
+    for _ in range(4):  # the first is a warm-up
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ev[0].record(st)
+        _, states = roe.forward_states(Ue, cs, steps)
+        ev[1].record(st)
+        roe.backward_states(states, gUTe, cs, steps)
+        ev[2].record(st)
+        torch.cuda.synchronize()
+        te.append((ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])))
+        del states
+    fe, be = min(t[0] for t in te[1:]), min(t[1] for t in te[1:])
+    del roe, Ue, UTe, gUTe
     # central difference in Cs on the FP64 path
     ro, U = r64["ro"], r64["U"]
     lo = lambda c: float(log_spectrum_misfit(ro.forward_states(U, c, steps)[0][..., : ro.nk], Et, n))
@@ -457,6 +477,8 @@ def bench_adjoint(rank):
            "grad_u0_rel_l2_f32_vs_f64": rel_l2(g32, g64),
            "rk3": {"fwd_ms": round(f3, 2), "bwd_ms": round(b3, 2), "adjoint_fwd_ratio": round(b3 / f3, 3),
                    "scheme": "the reference's RK3 (3 stages), FP32, same recipe"},
+           "etd2": {"fwd_ms": round(fe, 2), "bwd_ms": round(be, 2), "adjoint_fwd_ratio": round(be / fe, 3),
+                    "scheme": "corrected ETD2 (first step RK4), FP32, same recipe, every step's state kept"},
            "config": "128^3, random-phase spectrum k0=4, nu=2e-4, Smagorinsky Cs=0.17, RK4, dt=2e-3, 100 steps, "
                      "checkpoints every 10, loss on log E(k), k=1..43; backward = segment recompute + reverse stages"}
     del res, r32, r64, ro, U
