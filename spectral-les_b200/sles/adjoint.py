@@ -190,15 +190,20 @@ class ETD2Rollout:
     F(U_0) and runs RK4 (src/ETD2_method.py:7-14); later steps are
     U_{n+1} = E U_n + w1 F(U_n) + w0 F(U_{n-1}) with E = exp(-dt nu k^2) and
     F the explicit term (projected u x omega, LES stress, forcing).  The
-    forward keeps every step's input state for the reverse sweep, which runs
-    the ETD2 reverse steps on this plan and the first step's RK4 reverse on a
-    companion RK4 plan.  Same call and gradient conventions as ``RK4Rollout``.
+    forward keeps (U_n, F(U_{n-1})) every ``checkpoint_every`` steps; the
+    backward recomputes one segment at a time and runs the ETD2 reverse steps
+    on this plan and the first step's RK4 reverse on a companion RK4 plan.
+    Same call and gradient conventions as ``RK4Rollout``.
     """
 
-    def __init__(self, n, nu, dt, les="Smagorinsky", Cs=0.17, dtype=torch.float32, forcing=0.0, device="cuda"):
+    def __init__(self, n, nu, dt, les="Smagorinsky", Cs=0.17, dtype=torch.float32, forcing=0.0,
+                 checkpoint_every=10, device="cuda"):
+        if checkpoint_every < 1:
+            raise ValueError("checkpoint_every must be >= 1")
         self.rk = RK4Rollout(n, nu, dt, les=les, Cs=Cs, dtype=dtype, forcing=forcing, checkpoint_every=1,
                              device=device)
         self.n, self.nu, self.dt, self.forcing = self.rk.n, self.rk.nu, self.rk.dt, self.rk.forcing
+        self.every = int(checkpoint_every)
         self.rdtype, self.cdtype, self.device = self.rk.rdtype, self.rk.cdtype, self.rk.device
         self.plan = nat.Plan(3, self.n, dtype, self.rk.les, nat.SCHEME_ETD2, False, nu, Cs, forcing, self.device)
         autotune.apply_cached(self.plan, "ETD2")
@@ -209,44 +214,75 @@ class ETD2Rollout:
     def _new(self):
         return self.rk._new()
 
+    def _steps(self, U_start, F_prev, k0, k1, keep=None, ckpts=None):
+        """Steps k0 .. k1-1 from U_{k0} (F_prev = F(U_{k0-1}) when k0 >= 1);
+        appends each step's input state to ``keep`` and records checkpoints
+        (U_k, F(U_{k-1})) in ``ckpts``.  Returns U_{k1}."""
+        U = U_start.clone()
+        if k0 == 0:
+            F1, tmp = self._new(), self._new()
+            self.plan.rhs(U, tmp, F1)  # F(U_0), src/ETD2_method.py:8-14
+            if keep is not None:
+                keep.append(U.clone())
+            if ckpts is not None:
+                ckpts[0] = (U.clone(), None)
+            B, Cacc = self._new(), self._new()
+            self.rk._step(U, B, Cacc, False)  # first step: RK4
+            U, F0, k = B, tmp, 1
+        else:
+            F1, F0, k = F_prev.clone(), self._new(), k0
+        primed = False
+        while k < k1:
+            if keep is not None:
+                keep.append(U.clone())
+            if ckpts is not None and k % self.every == 0:
+                ckpts[k] = (U.clone(), F1.clone())
+            # U <- E U + w1 F(U) + w0 F1; F0 <- F(U) (src/ETD2_method.py:16-37)
+            self.plan.stage(0, self.dt, U, None, F1, U, F0, None, None, nat.STAGE_PRIMED if primed else 0)
+            primed = True
+            F0, F1 = F1, F0
+            k += 1
+        return U
+
     def forward_states(self, U0, Cs, nsteps):
-        """Run ``nsteps`` steps; return (U_T padded, [U_0 .. U_{T-1}] padded)."""
+        """Run ``nsteps`` steps; return (U_T padded, checkpoints)."""
         nsteps = int(nsteps)
         if nsteps < 1:
             raise ValueError("nsteps must be >= 1")
         for p in (self.plan, self.rk.plan):
             p.set_params(self.nu, Cs, self.forcing)
-        A = self.rk._pad(U0)
-        states = [A]
-        F1, tmp = self._new(), self._new()
-        self.plan.rhs(A, tmp, F1)  # F(U_0), src/ETD2_method.py:8-14
-        U, Cacc = self._new(), self._new()
-        self.rk._step(A, U, Cacc, False)  # first step: RK4
-        F0 = tmp
-        for k in range(1, nsteps):
-            states.append(U.clone())
-            # U <- E U + w1 F(U) + w0 F1; F0 <- F(U) (src/ETD2_method.py:16-37)
-            self.plan.stage(0, self.dt, U, None, F1, U, F0, None, None, nat.STAGE_PRIMED if k > 1 else 0)
-            F0, F1 = F1, F0
-        return U, states
+        ckpts = {}
+        U = self._steps(self.rk._pad(U0), None, 0, nsteps, ckpts=ckpts)
+        return U, ckpts
 
-    def backward_states(self, states, gUT, Cs, nsteps):
+    def backward_states(self, ckpts, gUT, Cs, nsteps):
         """Reverse sweep; returns (dL/dU_0 padded, dL/dCs float64 tensor)."""
         nsteps = int(nsteps)
-        self.plan.set_params(self.nu, Cs, self.forcing)
+        for p in (self.plan, self.rk.plan):
+            p.set_params(self.nu, Cs, self.forcing)
         csg = torch.zeros(1, dtype=torch.float64, device=self.device)
         ubar = self.rk._pad(gUT)
+        lam, acc = self._new(), self._new()
         if nsteps > 1:
-            lam, acc = self._new(), self._new()
             self.plan.adjoint_seed(self._ws, self.dt, ubar, acc, lam)  # lam = w1 ubar
-            self.plan.adjoint_prime(self._ws, states[nsteps - 1], lam)
-            for k in range(nsteps - 1, 0, -1):
-                # stage 0: a reverse ETD2 step; 1: the step after the RK4 step, which
-                # leaves lam = the cotangent of F(U_0) and primes at U_0
-                self.plan.adjoint_stage(self._ws, 0 if k > 1 else 1, self.dt, states[k - 1], ubar, acc, lam, csg)
+            starts = sorted(ckpts)
+            ends = starts[1:] + [nsteps]
+            for s0, s1 in reversed(list(zip(starts, ends))):
+                states = []  # U_{s0} .. U_{s1-1}
+                U_s, F_prev = ckpts[s0]
+                self._steps(U_s, F_prev, s0, s1, keep=states)
+                lo = max(s0, 1)
+                for k in range(s1 - 1, lo - 1, -1):
+                    if k == s1 - 1:
+                        self.plan.adjoint_prime(self._ws, states[k - s0], lam)
+                    un = states[k - 1 - s0] if k - 1 >= lo else None
+                    # stage 0: a reverse ETD2 step; 1: the step after the RK4 step, which
+                    # leaves lam = the cotangent of F(U_0)
+                    self.plan.adjoint_stage(self._ws, 0 if k > 1 else 1, self.dt, un, ubar, acc, lam, csg)
         # the RK4 step's reverse from dL/dU_1
-        g, c = self.rk.backward_states({0: states[0]}, ubar[..., : self.nk], Cs, 1)
+        g, c = self.rk.backward_states({0: ckpts[0][0]}, ubar[..., : self.nk], Cs, 1)
         if nsteps > 1:  # + J_F(U_0)^T (cotangent of F(U_0))
+            self.plan.adjoint_prime(self._ws, ckpts[0][0], lam)
             self.plan.adjoint_stage(self._ws, 2, self.dt, None, g, acc, lam, csg)
         return g, csg + c
 

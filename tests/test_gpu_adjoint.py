@@ -146,11 +146,11 @@ def test_adjoint_configuration_float32_against_float64():
     assert abs(c32 - c64) <= 1e-3 * abs(c64)
 
 
-@pytest.mark.parametrize("steps", [1, 2, 4])
+@pytest.mark.parametrize("steps,every", [(1, 10), (2, 10), (4, 10), (7, 3)])
 @pytest.mark.parametrize("les", ["Smagorinsky", "vreman", None])
-def test_etd2_rollout_matches_torch_autograd(les, steps):
+def test_etd2_rollout_matches_torch_autograd(les, steps, every):
     n, nu, dt, cs = 32, 3e-3, 5e-3, 0.17
-    ro = ETD2Rollout(n, nu, dt, les=les, Cs=cs, dtype=torch.float64)
+    ro = ETD2Rollout(n, nu, dt, les=les, Cs=cs, dtype=torch.float64, checkpoint_every=every)
     ps = PlainSolver(n, 3, nu=nu, dt=dt, les=les, Cs=cs, method="ETD2", parity=False, device="cuda")
     U0 = ps.rfft(_field(n, seed=8))
     g = torch.Generator(device="cuda").manual_seed(2)
@@ -177,7 +177,7 @@ def test_etd2_rollout_matches_torch_autograd(les, steps):
 
 def test_etd2_gradients_match_central_differences():
     n, nu, dt, cs, steps = 48, 2e-4, 2e-3, 0.17, 12
-    ro = ETD2Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=torch.float64)
+    ro = ETD2Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=torch.float64, checkpoint_every=5)
     U0 = ro.rfft(_field(n, seed=6))
     Et = shell_spectrum(U0, n).detach() * torch.linspace(0.8, 1.2, shell_spectrum(U0, n).numel(), device="cuda",
                                                          dtype=torch.float64)
