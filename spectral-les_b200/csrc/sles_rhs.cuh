@@ -274,7 +274,15 @@ struct XGeo {
 #endif
   static constexpr int NB =
       (XV == 0) ? 0 : ((BASE + (size_t)SLES_X_NB * TE * sizeof(C) <= BUDGET) ? SLES_X_NB : 0);
-  static constexpr size_t SMEM = BASE + (size_t)NB * TE * sizeof(C);
+  // XV 0: the stage's state tiles (ucur, u0) of one component prefetched with
+  // per-thread cp.async into two spare [N][W] buffers, while the item's
+  // forward transforms (component 0) or the previous component's inverse
+  // transforms run, where they fit the budget
+#ifndef SLES_X_SB
+#define SLES_X_SB 1
+#endif
+  static constexpr int SB = (SLES_X_SB && XV == 0 && BASE + (size_t)2 * TE * sizeof(C) <= BUDGET) ? 2 : 0;
+  static constexpr size_t SMEM = BASE + (size_t)(NB + SB) * TE * sizeof(C);
 };
 
 // slot of tile `i` in a pass's per-item load sequence
@@ -307,7 +315,7 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
   C* rst = reinterpret_cast<C*>(smem_raw);  // [D][N][W] projected components
   C* sm0 = rst + D * K::TE;                 // exchange scratch
   C* twt = sm0 + K::SCR;                    // twiddle table exp(-2 pi i e/N)
-  C* ring = twt + F::LIN_LEN;               // NB tile buffers [N][W]
+  C* ring = twt + F::LIN_LEN;               // NB tile buffers [N][W] (XV 0: SB state buffers)
   const StageCoef<Tp> SC = stage_coef<Tp>(A);
   const int tid = threadIdx.x;
   const int l = tid % W, j = tid / W;
@@ -410,6 +418,21 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
       }
       continue;
     }
+    // XV 0: prefetch component c's state tiles into the two spare buffers (each
+    // thread copies exactly the positions it later reads: no block barrier)
+    auto sissue = [&](int c) {
+      if constexpr (K::SB > 0) {
+        const long long so = c * fs + (long long)sl * A.nkp + (ok ? col : 0);
+        C* d0 = ring + j * W + l;
+#pragma unroll
+        for (int m = 0; m < V; ++m) {
+          if (A.need_uc) cp_async_el<sizeof(C)>(d0 + T * m * W, A.ucur + so + (j + T * m) * ps, ok);
+          if (A.need_u0) cp_async_el<sizeof(C)>(d0 + K::TE + T * m * W, A.u0 + so + (j + T * m) * ps, ok);
+        }
+        cp_async_commit();
+      }
+    };
+    sissue(0);
     // forward x-transforms; the x part of div(tau) joins in spectral space
 #pragma unroll 1
     for (int c = 0; c < D; ++c) {
@@ -468,11 +491,19 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
 #pragma unroll 1
     for (int c = 0; c < D; ++c) {
       C v[V];
-      C ucv[NB > 0 ? V : 1], u0v[NB > 0 ? V : 1], u1v[NB > 0 ? V : 1];
+      C ucv[NB > 0 || K::SB > 0 ? V : 1], u0v[NB > 0 || K::SB > 0 ? V : 1], u1v[NB > 0 ? V : 1];
       if constexpr (NB > 0) {
         if (A.need_uc) take(ucv, A.ucur, c);
         if (A.need_u0) take(u0v, A.u0, c);
         if (A.need_u1) take(u1v, A.u1, c);
+      } else if constexpr (K::SB > 0) {
+        cp_async_wait<0>();
+        const C* s0 = ring + j * W + l;
+#pragma unroll
+        for (int m = 0; m < V; ++m) {
+          ucv[m] = s0[T * m * W];
+          u0v[m] = s0[K::TE + T * m * W];
+        }
       }
       if (ok) {
 #pragma unroll
@@ -485,6 +516,10 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
             ucm = A.need_uc ? ucv[m] : cmk<C>(0, 0);
             u0m = A.need_u0 ? u0v[m] : ucm;
             u1m = A.need_u1 ? u1v[m] : cmk<C>(0, 0);
+          } else if constexpr (K::SB > 0) {
+            ucm = A.need_uc ? ucv[m] : cmk<C>(0, 0);
+            u0m = A.need_u0 ? u0v[m] : ucm;
+            u1m = A.need_u1 ? A.u1[c * fs + off] : cmk<C>(0, 0);
           } else {
             ucm = A.need_uc ? A.ucur[c * fs + off] : cmk<C>(0, 0);
             u0m = A.need_u0 ? A.u0[c * fs + off] : ucm;
@@ -496,6 +531,7 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
 #pragma unroll
         for (int m = 0; m < V; ++m) v[m] = cmk<C>(0, 0);
       }
+      if (c + 1 < D) sissue(c + 1);  // lands while this component's inverse transforms run
       if (A.prep) prep(c, v);
     }
   }
