@@ -41,6 +41,14 @@ def workload_name(n):
             "dt=%g, nu=%g, random-phase spectrum k0=%g u0=%g" % (n, CS, n, DT, NU, K0, U0))
 
 
+def bench_config(n, world):
+    """The workload description both arms print (identical dicts)."""
+    fbytes = float(n) * n * (n // 2 + 1) * 8
+    return {"workload": workload_name(n), "n": n, "scheme": "RK3 (reference arithmetic)", "les": "Smagorinsky",
+            "l2": "inputs larger than L2 (state 3x3x%.0f MB + workspace 9 fields at FP32)" % (fbytes / 1e6),
+            "parallelism": "replicas" if world > 1 else "single device"}
+
+
 def measured_peak():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -210,6 +218,10 @@ def bench_512(peak, rank):
     torch.cuda.empty_cache()
     v32, v64, vtp = npts * 20 / t32 / 1e6, npts * 20 / t64 / 1e6, npts / tp / 1e6
     ms = t32 / 20 * 1e3
+    names = ["x_inverse", "y_inverse", "z_fused", "y_forward", "x_forward_combine"]
+    fbytes = float(n) * n * (n // 2 + 1) * 8
+    algb = {"x_inverse": 9 * fbytes, "y_inverse": 15 * fbytes, "z_fused": 18 * fbytes, "y_forward": 15 * fbytes,
+            "x_forward_combine": 18 * fbytes}
     out["smagorinsky_rk3"] = {
         "value": round(v32, 2), "unit": UNIT, "ms_per_step": round(ms, 3),
         "fused_fp64_value": round(v64, 2), "torch_fft_fp64_value": round(vtp, 2),
@@ -218,8 +230,8 @@ def bench_512(peak, rank):
         "ek_err_fp32_vs_fp64_after_100_steps": {"max_rel_shells_above_1e-8_of_peak": ek, "up_to_shell": klive,
                                                 "max_rel_all_shells": ekall},
         "step_roofline_frac": round(STEP_BYTES_PER_PT_RHS["f32"] * 3 * npts / (ms * 1e-3) / 1e9 / peak, 4),
-        "kernel_ms": dict(zip(["x_inverse", "y_inverse", "z_fused", "y_forward", "x_forward_combine"],
-                              [round(x, 4) for x in kms])),
+        "kernel_ms": dict(zip(names, [round(x, 4) for x in kms])),
+        "kernel_gbs": {k: round(algb[k] / (t * 1e-3) / 1e9, 1) for k, t in zip(names, kms)},
         "autotune_fp32_fp64": tu,
         "config": "512^3, random-phase spectrum k0=4, nu=1e-4, Smagorinsky Cs=0.17, reference RK3, dt=1e-3"}
     # -- Vreman ETD2 at 512^3
@@ -369,6 +381,9 @@ def replicas_value(points_per_rank, steps, secs_local, world, device):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the oracle port of the reference's RK3 + Smagorinsky
+    path (float64 NumPy, scipy.fft with a worker per host core) on a bounded
+    sample of the same workload; its rate stands for the requested steps."""
     if rank != 0:
         return
     n = args.n
@@ -376,16 +391,78 @@ def run_reference(args, rank, world):
     w = min(args.warmup, 1)
     k = max(1, min(args.steps, 2))
     value, secs = cpu_oracle_rate(n, k, w, 0, cores)
-    sample = ("%d timed RK3 step(s) at %d^3 after %d warm-up step(s) of the requested %d/%d; oracle port "
-              "(NumPy + scipy.fft workers=%d) on the host cores" % (k, n, w, args.steps, args.warmup, cores))
+    sample = ("%d timed RK3 step(s) at %d^3 after %d warm-up step(s); the rate stands for the requested %d "
+              "steps (%.0f s at %.1f s/step, extrapolated); oracle port (NumPy + scipy.fft workers=%d) on the "
+              "host cores; the reference itself needs mpi4py/mpi4py-fft, absent on this image" %
+              (k, n, w, args.steps, secs / k * args.steps, secs / k, cores))
     out = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
-           "steps": k, "warmup": w, "ms_per_step": round(secs / k * 1e3, 2), "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, seed 0)",
-           "config": {"workload": workload_name(n), "n": n, "scheme": "RK3 (reference)", "les": "Smagorinsky"},
+           "steps": k, "steps_requested": args.steps, "warmup": w, "ms_per_step": round(secs / k * 1e3, 2),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded random-phase spectrum, seed=rank)", "config": bench_config(n, world),
            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "port",
                             "sample": sample},
            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
+
+
+def bench_fft(rank):
+    """The project's batched 3D r2c / c2r (sles_fft_r2c / sles_fft_c2r, 3
+    fields) against torch.fft.rfftn / irfftn (cuFFT) on the same 3 fields, at
+    256^3 and 512^3 in float32 and float64: mean ms per call (CUDA events, 10
+    calls after 3 warm-up calls) and the effective HBM rate of a two-pass
+    out-of-cache transform model (real read + half-complex written, twice)."""
+    import torch
+    from sles import _native as nat
+    out = {}
+    for n in (256, 512):
+        for dt in (torch.float32, torch.float64):
+            tag = "%d_%s" % (n, "f32" if dt == torch.float32 else "f64")
+            plan = nat.Plan(3, n, dt, nat.LES_NONE, nat.SCHEME_RK4, True, 0.0, 0.0, 0.0, "cuda")
+            g = torch.Generator(device="cuda").manual_seed(rank)
+            x = torch.randn((3, n, n, n), dtype=dt, device="cuda", generator=g)
+            cd = torch.complex64 if dt == torch.float32 else torch.complex128
+            hc = torch.empty((3, n, n, plan.nkp), dtype=cd, device="cuda")
+            y = torch.empty_like(x)
+
+            def timeit(fn, reps=10):
+                for _ in range(3):
+                    fn()
+                st = torch.cuda.current_stream()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(st)
+                for _ in range(reps):
+                    fn()
+                e1.record(st)
+                torch.cuda.synchronize()
+                return e0.elapsed_time(e1) / reps
+
+            r = {"sles_r2c_ms": timeit(lambda: plan.fft_r2c(x, hc, 3)),
+                 "sles_c2r_ms": timeit(lambda: plan.fft_c2r(hc, y, 3))}
+            err_rt = float(torch.linalg.vector_norm(y - x) / torch.linalg.vector_norm(x))
+            ref = torch.fft.rfftn(x, dim=(1, 2, 3))
+            err_f = float(torch.linalg.vector_norm(hc[..., : n // 2 + 1] - ref) / torch.linalg.vector_norm(ref))
+            del ref
+            r["cufft_rfftn_ms"] = timeit(lambda: torch.fft.rfftn(x, dim=(1, 2, 3)))
+            h2 = torch.fft.rfftn(x, dim=(1, 2, 3))
+            r["cufft_irfftn_ms"] = timeit(lambda: torch.fft.irfftn(h2, s=(n, n, n), dim=(1, 2, 3)))
+            del h2
+            esz = 4 if dt == torch.float32 else 8
+            model = 3 * 2 * (float(n) ** 3 * esz + float(n) * n * (n // 2 + 1) * 2 * esz)
+            for k in ("sles_r2c_ms", "sles_c2r_ms", "cufft_rfftn_ms", "cufft_irfftn_ms"):
+                r[k] = round(r[k], 4)
+            r["sles_r2c_gbs"] = round(model / (r["sles_r2c_ms"] * 1e-3) / 1e9, 1)
+            r["cufft_rfftn_gbs"] = round(model / (r["cufft_rfftn_ms"] * 1e-3) / 1e9, 1)
+            r["speedup_r2c_vs_cufft"] = round(r["cufft_rfftn_ms"] / r["sles_r2c_ms"], 3)
+            r["speedup_c2r_vs_cufft"] = round(r["cufft_irfftn_ms"] / r["sles_c2r_ms"], 3)
+            r["rel_err_r2c_vs_cufft"] = err_f
+            r["rel_err_roundtrip"] = err_rt
+            out[tag] = r
+            del x, y, hc, plan
+            torch.cuda.empty_cache()
+    out["note"] = ("3 fields per call; the project's transforms are the unfused standalone passes (r2c lines, "
+                   "then c2c along y and x); the fused RHS never runs them")
+    return out
 
 
 def bench_adjoint(rank):
@@ -581,6 +658,62 @@ def bench_ensemble(rank, steps=200):
     return out
 
 
+def bench_steps(case, n, precision, steps, warmup, rank, xvar=-1):
+    """A plain stepping run of one workload (for ncu launch lists and
+    captures): the Smagorinsky recipe with the reference RK3 or RK4, or the
+    Vreman case with the corrected ETD2, at n^3."""
+    from sles import ETD2_method, RK3_method, RK4_method
+    if case == "vreman_etd2":
+        d = make_domain(n, precision, rank, method="ETD2", les="vreman", nu=5e-5, cs=math.sqrt(0.07 / 2.5), dt=5e-4,
+                        k0=6.0, parity=False)
+        step = ETD2_method.solveForNextTimestep
+    elif case == "smag_rk4":
+        d = make_domain(n, precision, rank, method="RK4")
+        d.U_hat1[...] = d.U_hat
+        step = RK4_method.solveForNextTimestep
+    else:
+        d = make_domain(n, precision, rank)
+        step = RK3_method.solveForNextTimestep
+    if xvar >= 0:
+        d._plan.set_variant(xvar)
+    for _ in range(warmup):
+        step(d)
+    secs = time_steps(d, steps, step)
+    d._plan.check()
+    return {"case": case, "n": n, "precision": precision, "steps": steps, "ms_per_step": round(secs / steps * 1e3, 4),
+            "x_variant": d._plan.get_variant(0)}
+
+
+def north_star_summary(out):
+    """The headline figures in a few hundred characters (printed last)."""
+    r = lambda x, k=4: None if x is None else (round(x, k) if isinstance(x, float) else x)
+    ns = {"fp32_256": out["value"], "roofline_frac": out["roofline"]["frac"],
+          "step_model_frac": out["step_roofline"]["frac"], "e2e_256": out["e2e"]["value"]}
+    if "fp64" in out:
+        f = out["fp64"]
+        ns.update(fp64_fused_256=f["fused_fp64_value"], fp64_torch_256=f["torch_fft_fp64_value"],
+                  fp32_vs_fp64_rel_l2=r(f["rel_l2_fp32_vs_fp64"], 10),
+                  fp64_fused_vs_cpu_fp64=f.get("fused_fp64_vs_cpu_fp64"))
+    if "n512" in out:
+        a, b = out["n512"]["smagorinsky_rk3"], out["n512"]["vreman_etd2"]
+        ns["n512_smag_rk3"] = {"value": a["value"], "x_torch_fp64": a["speedup_vs_torch_fp64"],
+                               "rel_l2_100": r(a["rel_l2_fp32_vs_fp64_after_100_steps"], 10),
+                               "ek_err_100": r(a["ek_err_fp32_vs_fp64_after_100_steps"][
+                                   "max_rel_shells_above_1e-8_of_peak"], 8),
+                               "step_model_frac": a["step_roofline_frac"], "kernel_gbs": a.get("kernel_gbs")}
+        ns["n512_vreman_etd2"] = {"value": b["value"], "rel_l2_100": r(b["rel_l2_fp32_vs_fp64_after_100_steps"], 10),
+                                  "step_model_frac": b["step_roofline_frac"]}
+    if "adjoint" in out:
+        ns["adjoint_fwd_ratio"] = out["adjoint"]["adjoint_fwd_ratio"]
+        ns["adjoint_cs_rel_err"] = r(out["adjoint"]["cs_rel_err_f64_vs_richardson"], 12)
+    if "ensemble" in out:
+        ns["ensemble_x_seq"] = out["ensemble"]["speedup_vs_sequential"]
+    if "fft_vs_cufft" in out:
+        ns["fft_r2c_x_cufft"] = {k: v["speedup_r2c_vs_cufft"] for k, v in out["fft_vs_cufft"].items()
+                                 if isinstance(v, dict)}
+    return ns
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -592,8 +725,13 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (use the default or cached kernel variants)")
-    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble", "driver"],
-                    help="run one extra block alone and print it (profiling; not a bench line)")
+    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble", "driver", "fft", "steps"],
+                    help="run one extra block alone and print it (profiling; not a bench line); 'steps': "
+                         "--case at --n stepped --steps times after --warmup (for ncu launch lists)")
+    ap.add_argument("--case", default="smag_rk3", choices=["smag_rk3", "vreman_etd2", "smag_rk4"],
+                    help="workload of --only steps")
+    ap.add_argument("--precision", default="float32", choices=["float32", "float64"])
+    ap.add_argument("--xvar", type=int, default=-1, help="x-pass variant of --only steps (-1: default/cached)")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference", "at least 3 warm-up steps"
     global TUNE
@@ -628,7 +766,10 @@ def main():
     if args.only:
         peak, _ = measured_peak()
         fn = {"n512": lambda: bench_512(peak, rank), "adjoint": lambda: bench_adjoint(rank),
-              "ensemble": lambda: bench_ensemble(rank), "driver": lambda: bench_driver(rank)}[args.only]
+              "ensemble": lambda: bench_ensemble(rank), "driver": lambda: bench_driver(rank),
+              "fft": lambda: bench_fft(rank),
+              "steps": lambda: bench_steps(args.case, args.n, args.precision, args.steps, args.warmup, rank,
+                                           args.xvar)}[args.only]
         print(json.dumps({"only": args.only, "result": fn()}))
         return
 
@@ -658,7 +799,7 @@ def main():
     # = half-complex fields read + written per launch
     rinfo = {"z_fused": (18, "k_zpass_f32_%d_smag" % n,
                          "k_zpass (fused z pass: c2r x12, u x omega, Smagorinsky stress, r2c x9)"),
-             "x_forward_combine": (18, "k_xpass_f32_%d_smag_rhs" % n,
+             "x_forward_combine": (18, "k_xpass_f32_%d_smag_rhs_xv%d" % (n, d._plan.get_variant(0)),
                                    "k_xpass (x forward of 6 slots, kx stress part, mask, projection, viscous "
                                    "term, update, x inverse priming the next RHS; 9 fields in, 9 out)")}
     dom = max(rinfo, key=lambda k: kms[names.index(k)])
@@ -678,7 +819,7 @@ def main():
     host_out = torch.empty_like(host_in, pin_memory=True)
     host_in.copy_(d.U_hat)
     torch.cuda.synchronize()
-    ke = max(10, args.steps // 4)
+    ke = max(40, args.steps)
     hs = HostStepper(d, steps=1)
     hs.run(host_in, [host_out] * 2)
     hs.synchronize()
@@ -699,10 +840,8 @@ def main():
     out = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random-phase spectrum, seed=rank)",
-           "config": {"workload": workload_name(n), "n": n, "scheme": "RK3 (reference arithmetic)",
-                      "les": "Smagorinsky", "precision": "fp32 fields/FFTs, fp64 twiddles",
-                      "l2": "inputs larger than L2 (state 3x3x%.0f MB + workspace 9 fields)" % (fbytes / 1e6),
-                      "parallelism": "replicas" if world > 1 else "single GPU", "autotune": tuned},
+           "config": bench_config(n, world),
+           "precision": "fp32 fields/FFTs, fp64 twiddles", "autotune": tuned,
            "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": io_bytes,
                    "d2h_bytes_per_step": io_bytes, "steps": ke,
                    "path": "sles.pipeline.HostStepper: per step pinned host -> U_hat, RK3_method."
@@ -715,7 +854,10 @@ def main():
            "step_roofline": {"model_bytes_per_step": step_alg, "achieved": round(step_ach, 1), "unit": "GB/s",
                              "frac": round(step_ach / peak, 4),
                              "model": "384 B/pt/RHS x 3 RHS/step (21 transforms x 16 B + 48 B state)"},
-           "kernel_ms": kdict}
+           "kernel_ms": kdict,
+           "kernel_gbs": {k: round(b_ * fbytes / (kms[names.index(k)] * 1e-3) / 1e9, 1) for k, b_ in
+                          (("x_inverse", 9), ("y_inverse", 15), ("z_fused", 18), ("y_forward", 15),
+                           ("x_forward_combine", 18))}}
 
     # ---------------- FP64 comparisons ----------------
     if not args.no_compare:
@@ -745,6 +887,7 @@ def main():
                                                "max_rel_all_shells": ekall},
                        "note": "FP32 fused vs FP64 fused (same kernels, float64) on the same seeded field"}
     if not args.no_compare and world == 1:
+        out["fft_vs_cufft"] = bench_fft(rank)
         out["n512"] = bench_512(peak, rank)
         adj = bench_adjoint(rank)
         out["adjoint"] = adj
@@ -761,7 +904,10 @@ def main():
         out["cpu_baseline"] = {"value": round(v_cpu, 4), "unit": UNIT, "cores": cores, "kind": "port",
                                "sample": "1 RK3 step at %d^3 (%.1f s), NumPy + scipy.fft workers=%d" %
                                          (n, secs_cpu, cores)}
+        if "fp64" in out:  # precision-matched: the fused float64 path against the float64 CPU port
+            out["fp64"]["fused_fp64_vs_cpu_fp64"] = round(out["fp64"]["fused_fp64_value"] / v_cpu, 1)
     out["clocks"] = clk.summary()
+    out["north_star"] = north_star_summary(out)  # last: the compact figures stay in a short stdout tail
     if rank == 0:
         print(json.dumps(out))
     if world > 1:

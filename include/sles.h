@@ -194,7 +194,10 @@ int sles_profile_rhs(sles_plan* plan, const void* u_hat, void* du_scratch, int i
  * SLES_ERR_WORKSPACE before anything runs (e.g. 3D LES up to N = 64 in float64,
  * N = 64 in float32; 3D without LES and 2D go further).
  * The first call on a device looks up the array's device address with that
- * device current; make that first call before any stream capture.  Every GPU
+ * device current; make that first call before any stream capture.  The
+ * address is kept per device together with the CUDA context it belongs to and
+ * looked up again when the current context differs (after cudaDeviceReset the
+ * array's old contents are gone with the context).  Every GPU
  * that loads the library holds the array until the process exits.  All calls on
  * a device share the array and it keeps the last call's contents (each call
  * clears the part that must start at zero); calls whose work overlaps on the
@@ -204,6 +207,18 @@ int sles_profile_rhs(sles_plan* plan, const void* u_hat, void* du_scratch, int i
 #define SLES_STATIC_WORKSPACE_BYTES (32u << 20)
 int sles_rhs_static_workspace(sles_plan* plan, const void* u_hat, const void* u_phys, const void* curl_phys,
                               void* du_out, void* f1_out, void* stream);
+/*
+ * Error word of the static array of the current device (no counterpart in the
+ * reference): as sles_plan_check, for calls of sles_rhs_static_workspace,
+ * whose bounded waits report there.  Synchronises `stream`, stores the word in
+ * *flags_out (may be NULL), clears it, returns SLES_ERR_TIMEOUT /
+ * SLES_ERR_NONFINITE when such a bit was set.  Check after the calls and
+ * before the next one (each call clears the word when it starts).
+ * sles_static_workspace_selftest_timeout makes a short bounded wait on that
+ * word run out, to exercise the path.
+ */
+int sles_static_workspace_check(unsigned* flags_out, void* stream);
+int sles_static_workspace_selftest_timeout(void* stream);
 
 /*
  * Discrete adjoint of the RK4 step (3D; no counterpart in the reference): the
@@ -256,6 +271,9 @@ int sles_rhs_static_workspace(sles_plan* plan, const void* u_hat, const void* u_
  * SLES_ERR_UNSUPPORTED.
  */
 size_t sles_adjoint_workspace_bytes(const sles_plan* plan);
+/* Error word of an adjoint workspace (its header, written by the reverse
+ * passes' bounded waits and non-finite checks): as sles_plan_check. */
+int sles_adjoint_check(sles_plan* plan, void* adj_ws, unsigned* flags_out, void* stream);
 int sles_adjoint_seed(sles_plan* plan, void* adj_ws, double dt, const void* ubar, void* acc, void* lam,
                       void* stream);
 int sles_adjoint_prime(sles_plan* plan, void* adj_ws, const void* u_state, const void* lam, void* stream);
@@ -315,6 +333,9 @@ int sles_stage_ctl(sles_plan* plan, int stage, void* dtctl, int parity, const vo
  */
 int sles_plan_check(sles_plan* plan, unsigned* flags_out, void* stream);
 int sles_selftest_wait_timeout(sles_plan* plan, void* stream);
+/* The same self-test against any device error word (e.g. an adjoint
+ * workspace's header; 4-byte aligned device pointer). */
+int sles_selftest_wait_timeout_word(void* word_dev, void* stream);
 /* Human-readable text for a status code (static storage). */
 const char* sles_status_string(int status);
 int sles_version(void);

@@ -40,7 +40,8 @@ __all__ = [
     "etd2_step", "step", "initial_velocity", "initial_vorticity",
     "taylor_green", "random_spectrum_velocity", "gaussian_vorticity_2d",
     "energy", "dissipation", "shell_spectrum", "reference_binned_spectrum",
-    "etd2_coefficients", "set_fft_workers",
+    "etd2_coefficients", "set_fft_workers", "U_square", "dissipation_rate", "compute_dt",
+    "solver_loop",
 ]
 
 _FFT_WORKERS = None  # None -> numpy.fft (pocketfft, 1 thread); int -> scipy.fft workers
@@ -590,3 +591,75 @@ def reference_binned_spectrum(d, U_hat=None):
             tk[i] = np.mean(np.sqrt(d.K2[sel]))
             tE[i] = np.mean(Ek[sel])
     return tk, tE
+
+
+def U_square(d):
+    """sum_i mean(u_i^2) over the physical field (no 1/2): src/RK4_method.py:77-84."""
+    U = np.array([bwd(d.U_hat[i], d.dim, d.N) for i in range(d.dim)])
+    return float(np.sum(U * U)) / float(d.N) ** d.dim
+
+
+def dissipation_rate(d):
+    """nu * sum_i sum_x u_i irfftn(K^2 U_hat_i) (a sum, not a mean):
+    src/RK4_method.py:87-101."""
+    eps = 0.0
+    for i in range(d.dim):
+        u = bwd(d.U_hat[i], d.dim, d.N)
+        eps += d.nu * float(np.sum(u * bwd(d.U_hat[i] * d.K2, d.dim, d.N)))
+    return eps
+
+
+# ---------------------------------------------------------------------------
+# driver loop (src/SM_solver.py)
+# ---------------------------------------------------------------------------
+
+def compute_dt(u_max, nu, dx, CFL):
+    """dt = min(CFL dx/u_max, 0.1 dx^2/nu); the reference exits below 1e-6
+    (src/SM_solver.py:258-277).  Raises SystemExit there."""
+    dt1 = CFL * dx / u_max
+    dt2 = 0.1 * dx ** 2 / nu if nu > 0 else 1e6
+    dt = min(dt1, dt2)
+    if dt < 1e-6:
+        raise SystemExit(1)
+    return dt
+
+
+def solver_loop(d, final_time, CFL=0.5, No_Ek_plot=5):
+    """The loop of spectralMethodSolver (src/SM_solver.py:18-83) without file
+    output: u_max = max over components and points of U (signed,
+    find_max_velocity :245-255), dt from compute_dt with CFL 0.3 before the
+    first step, t starts at dt_0, E(k) snapshots (width-5 bins) whenever
+    t >= the next multiple of final_time/No_Ek_plot, stop at t >= final_time
+    or dt < 1e-8, NaN stop.  Returns (steps, dt list, u_max list, snapshots)
+    with snapshots = [(t, temp_k, temp_Ek)]."""
+    dts, umaxs, snaps = [], [], []
+
+    def umax():
+        return float(np.max(d.U))  # the stored physical velocity, as the reference reads domain.U
+
+    u = umax()
+    d.dt = compute_dt(u, d.nu, d.dx, 0.3)
+    dts.append(d.dt)
+    umaxs.append(u)
+    t = d.dt
+    interval = final_time / No_Ek_plot if No_Ek_plot != 0 else 0
+    counter_t = 0.0
+    d.U_hat1 = d.U_hat.copy()
+    steps = 0
+    while True:
+        if interval > 0 and t >= counter_t:
+            tk, tE = reference_binned_spectrum(d)
+            snaps.append((t, tk, tE))
+            counter_t += interval
+        if t >= final_time or d.dt < 1e-8:
+            break
+        t += d.dt
+        step(d)
+        steps += 1
+        u = umax()
+        d.dt = compute_dt(u, d.nu, d.dx, CFL)
+        dts.append(d.dt)
+        umaxs.append(u)
+        if d.dt != d.dt:
+            break
+    return steps, dts, umaxs, snaps

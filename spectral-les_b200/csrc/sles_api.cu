@@ -201,23 +201,39 @@ int sles_stage_ctl(sles_plan* p, int stage, void* dtctl, int parity, const void*
                        reinterpret_cast<sles_dtctl*>(dtctl), parity);
 }
 
-int sles_plan_check(sles_plan* p, unsigned* flags_out, void* stream) {
-  if (int s = ready(p)) return s;
+}  // extern "C"
+
+namespace {
+// Copy a device error word to the host, clear it and map its bits to a status.
+int read_clear_flags(unsigned* word, unsigned* flags_out, cudaStream_t st) {
   unsigned w = 0;
-  cudaStream_t st = (cudaStream_t)stream;
-  if (cudaMemcpyAsync(&w, p->info.flags, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+  if (cudaMemcpyAsync(&w, word, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return SLES_ERR_CUDA;
   if (flags_out) *flags_out = w;
-  if (w && cudaMemsetAsync(p->info.flags, 0, sizeof(unsigned), st) != cudaSuccess) return SLES_ERR_CUDA;
+  if (w && cudaMemsetAsync(word, 0, sizeof(unsigned), st) != cudaSuccess) return SLES_ERR_CUDA;
   if (w & sles::SLES_ERRF_WAIT_TIMEOUT) return SLES_ERR_TIMEOUT;
   if (w & sles::SLES_ERRF_NONFINITE) return SLES_ERR_NONFINITE;
   return SLES_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int sles_plan_check(sles_plan* p, unsigned* flags_out, void* stream) {
+  if (int s = ready(p)) return s;
+  return read_clear_flags(p->info.flags, flags_out, (cudaStream_t)stream);
 }
 
 int sles_selftest_wait_timeout(sles_plan* p, void* stream) {
   if (int s = ready(p)) return s;
   return sles::launch(sles::k_wait_selftest, 1, 32, 0, (cudaStream_t)stream, p->info.flags, 4096L);
+}
+
+int sles_selftest_wait_timeout_word(void* word, void* stream) {
+  if (!word || ((uintptr_t)word) % sizeof(unsigned) != 0) return SLES_ERR_INVALID_ARG;
+  return sles::launch(sles::k_wait_selftest, 1, 32, 0, (cudaStream_t)stream, reinterpret_cast<unsigned*>(word),
+                      4096L);
 }
 
 int sles_diag(sles_plan* p, const void* uh, const void* uphys, double* out, double* spectrum, int nshell,
@@ -251,6 +267,12 @@ static int adjoint_info(sles_plan* p, void* adj_ws, sles::PlanInfo* out) {
   out->flags = reinterpret_cast<unsigned*>(adj_ws);
   out->scal = reinterpret_cast<double*>(reinterpret_cast<char*>(adj_ws) + 256);
   return SLES_OK;
+}
+
+int sles_adjoint_check(sles_plan* p, void* adj_ws, unsigned* flags_out, void* stream) {
+  sles::PlanInfo I;
+  if (int s = adjoint_info(p, adj_ws, &I)) return s;
+  return read_clear_flags(I.flags, flags_out, (cudaStream_t)stream);
 }
 
 int sles_adjoint_seed(sles_plan* p, void* adj_ws, double dt, const void* ubar, void* acc, void* lam, void* stream) {
@@ -294,7 +316,53 @@ static __device__ __align__(256) unsigned char g_sles_static_ws[SLES_STATIC_WORK
 namespace {
 std::mutex g_static_ws_mu;
 constexpr int kMaxDevices = 64;
-void* g_static_ws_addr[kMaxDevices] = {};  // device address of g_sles_static_ws, per device ordinal
+// device address of g_sles_static_ws per device ordinal, with the CUDA context
+// it was looked up in: after a device reset (or in another context) the
+// address is looked up again
+struct StaticAddr {
+  void* ctx;
+  void* addr;
+};
+StaticAddr g_static_ws_addr[kMaxDevices] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(f);
+  });
+  return fn;
+}
+
+// The array's device address on the current device (in host code the array's
+// name is only a host-side stand-in, so it is looked up with the device
+// current).  Makes no allocation.
+int static_ws_address(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return SLES_ERR_CUDA;
+  if (dev < 0 || dev >= kMaxDevices) return SLES_ERR_UNSUPPORTED;
+  CtxGetCurrentFn getctx = ctx_get_current();
+  if (!getctx) return SLES_ERR_CUDA;
+  CUcontext ctx = nullptr;
+  if (getctx(&ctx) != CUDA_SUCCESS) return SLES_ERR_CUDA;
+  std::lock_guard<std::mutex> g(g_static_ws_mu);
+  StaticAddr& e = g_static_ws_addr[dev];
+  if (!e.addr || !ctx || e.ctx != (void*)ctx) {
+    void* a = nullptr;
+    if (cudaGetSymbolAddress(&a, g_sles_static_ws) != cudaSuccess || !a) return SLES_ERR_CUDA;
+    // the lookup makes the device's context current if none was
+    if (getctx(&ctx) != CUDA_SUCCESS || !ctx) return SLES_ERR_CUDA;
+    e.addr = a;
+    e.ctx = (void*)ctx;
+  }
+  *out = e.addr;
+  return SLES_OK;
+}
 }  // namespace
 
 extern "C" int sles_rhs_static_workspace(sles_plan* p, const void* uh, const void* uphys, const void* cphys,
@@ -302,21 +370,8 @@ extern "C" int sles_rhs_static_workspace(sles_plan* p, const void* uh, const voi
   if (!p || !uh || !du) return SLES_ERR_INVALID_ARG;
   if (sles_plan_workspace_bytes(p) > (size_t)SLES_STATIC_WORKSPACE_BYTES) return SLES_ERR_WORKSPACE;
   if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return SLES_ERR_CUDA;
-  if (dev < 0 || dev >= kMaxDevices) return SLES_ERR_UNSUPPORTED;
   void* ws = nullptr;
-  {
-    // first call on a device: look up the array's device address with that
-    // device current (in host code the array's name is only a host-side stand-in)
-    std::lock_guard<std::mutex> g(g_static_ws_mu);
-    if (!g_static_ws_addr[dev]) {
-      void* a = nullptr;
-      if (cudaGetSymbolAddress(&a, g_sles_static_ws) != cudaSuccess || !a) return SLES_ERR_CUDA;
-      g_static_ws_addr[dev] = a;
-    }
-    ws = g_static_ws_addr[dev];
-  }
+  if (int s = static_ws_address(&ws)) return s;
   sles::PlanInfo info = p->info;  // the plan's own workspace (if any) is left untouched
   info.ws = ws;
   info.ws_bytes = SLES_STATIC_WORKSPACE_BYTES;
@@ -324,4 +379,16 @@ extern "C" int sles_rhs_static_workspace(sles_plan* p, const void* uh, const voi
   info.scal = reinterpret_cast<double*>(reinterpret_cast<char*>(ws) + 256);
   if (cudaMemsetAsync(info.flags, 0, sizeof(unsigned), (cudaStream_t)stream) != cudaSuccess) return SLES_ERR_CUDA;
   return p->eng->rhs(info, uh, uphys, cphys, du, f1, (cudaStream_t)stream);
+}
+
+extern "C" int sles_static_workspace_check(unsigned* flags_out, void* stream) {
+  void* ws = nullptr;
+  if (int s = static_ws_address(&ws)) return s;
+  return read_clear_flags(reinterpret_cast<unsigned*>(ws), flags_out, (cudaStream_t)stream);
+}
+
+extern "C" int sles_static_workspace_selftest_timeout(void* stream) {
+  void* ws = nullptr;
+  if (int s = static_ws_address(&ws)) return s;
+  return sles::launch(sles::k_wait_selftest, 1, 32, 0, (cudaStream_t)stream, reinterpret_cast<unsigned*>(ws), 4096L);
 }

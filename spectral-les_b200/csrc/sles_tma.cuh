@@ -63,6 +63,17 @@ struct TileRing {
     for (int k = 0; k < nbox; ++k)
       tma_load_4d(dst + (long long)k * (TE / nbox), map, c0, k * rows_per_box, slice, slot, b);
   }
+  // thread 0: the same with the box rows along the slice axis (dim 2) at the
+  // fixed row `row` (dim 1): x-pass tiles [x][W] at one ky
+  __device__ __forceinline__ void issue_rows(long long t, const CUtensorMap* map, int c0, int row, int slot,
+                                             int nbox, int rows_per_box, unsigned box_bytes) {
+    uint64_t* b = &bar[t % NBUF];
+    C* dst = tile(t);
+    fence_proxy_async();
+    mbar_arrive_expect_tx(b, box_bytes * nbox);
+    for (int k = 0; k < nbox; ++k)
+      tma_load_4d(dst + (long long)k * (TE / nbox), map, c0, row, k * rows_per_box, slot, b);
+  }
   __device__ __forceinline__ void wait(long long t, unsigned* err) {
     mbar_wait_bounded(&bar[t % NBUF], (unsigned)((t / NBUF) & 1), err);
   }

@@ -27,7 +27,8 @@ EXPORTED = [
     "sles_status_string", "sles_version", "sles_profile_rhs", "sles_rhs_static_workspace",
     "sles_adjoint_workspace_bytes", "sles_adjoint_seed", "sles_adjoint_prime", "sles_adjoint_stage",
     "sles_plan_variant_count", "sles_plan_get_variant", "sles_plan_set_variant", "sles_stage_ctl",
-    "sles_plan_check", "sles_selftest_wait_timeout",
+    "sles_plan_check", "sles_selftest_wait_timeout", "sles_selftest_wait_timeout_word", "sles_adjoint_check",
+    "sles_static_workspace_check", "sles_static_workspace_selftest_timeout",
 ]
 DT_DONE, DT_SNAPSHOT, DT_NAN, DT_TOO_SMALL = 1, 2, 4, 8
 
@@ -95,6 +96,10 @@ def load_library(path: str = LIB_PATH):
         "sles_stage_ctl": (i, [vp, i, vp, i, vp, vp, vp, vp, vp, vp, vp, i, vp]),
         "sles_plan_check": (i, [vp, ctypes.POINTER(ctypes.c_uint), vp]),
         "sles_selftest_wait_timeout": (i, [vp, vp]),
+        "sles_selftest_wait_timeout_word": (i, [vp, vp]),
+        "sles_adjoint_check": (i, [vp, vp, ctypes.POINTER(ctypes.c_uint), vp]),
+        "sles_static_workspace_check": (i, [ctypes.POINTER(ctypes.c_uint), vp]),
+        "sles_static_workspace_selftest_timeout": (i, [vp]),
         "sles_plan_variant_count": (i, [vp, i]),
         "sles_plan_get_variant": (i, [vp, i]),
         "sles_plan_set_variant": (i, [vp, i, i]),
@@ -231,6 +236,14 @@ class Plan:
         with torch.cuda.device(self.device):
             t = torch.zeros(nbytes + 256, dtype=torch.uint8, device=self.device)
         return t, t.data_ptr() + (-t.data_ptr()) % 256
+
+    def adjoint_check(self, ws_ptr):
+        """As check(), for the adjoint workspace's error word: raises SlesError
+        if a reverse pass's bounded wait gave up or saw a non-finite value."""
+        w = ctypes.c_uint(0)
+        check(self.L.sles_adjoint_check(self.h, ctypes.c_void_p(ws_ptr), ctypes.byref(w), stream_handle(self.device)),
+              "sles_adjoint_check")
+        return int(w.value)
 
     def adjoint_seed(self, ws_ptr, dt, ubar, acc, lam):
         check(self.L.sles_adjoint_seed(self.h, ctypes.c_void_p(ws_ptr), float(dt), ptr(ubar), ptr(acc), ptr(lam),

@@ -156,6 +156,9 @@ class RK4Rollout:
                     else:
                         un = states(i - 1, last) if i > 0 else None
                     self.plan.adjoint_stage(self._ws, s, dt, un, ubar, acc, lam, csg)
+        # a bounded wait that gave up (forward recompute or reverse passes) raises here
+        self.plan.check()
+        self.plan.adjoint_check(self._ws)
         return ubar, csg
 
     def __call__(self, U0, Cs, nsteps):
@@ -284,6 +287,8 @@ class ETD2Rollout:
         if nsteps > 1:  # + J_F(U_0)^T (cotangent of F(U_0))
             self.plan.adjoint_prime(self._ws, ckpts[0][0], lam)
             self.plan.adjoint_stage(self._ws, 2, self.dt, None, g, acc, lam, csg)
+        self.plan.check()
+        self.plan.adjoint_check(self._ws)
         return g, csg + c
 
     def __call__(self, U0, Cs, nsteps):

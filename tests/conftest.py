@@ -15,5 +15,17 @@ for p in (REPO, PKG_ROOT):
 GOLDEN = os.path.join(REPO, "tests", "golden")
 
 
+def step_cases():
+    """Fixtures of fixed-dt integrator runs (the others hold operator,
+    diagnostic or driver-loop records)."""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN)
+                  if f.endswith(".npz") and not f.startswith(("ops", "diag", "solver_")))
+
+
+def solver_cases():
+    """Fixtures of the reference's driver loop (spectralMethodSolver)."""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.startswith("solver_") and f.endswith(".npz"))
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")

@@ -1,6 +1,8 @@
 """Failure detection without a GPU fault: a kernel whose wait runs out (an
 mbarrier that nothing arrives at) reports SLES_ERR_TIMEOUT through the plan's
 error word, and the context stays usable."""
+import ctypes
+
 import pytest
 import torch
 
@@ -27,3 +29,18 @@ def test_wait_timeout_is_reported_and_context_survives():
         RK3_method.solveForNextTimestep(d)
     assert d._plan.check() == 0
     assert bool(torch.isfinite(d.U_hat.abs()).all())
+
+
+def test_adjoint_workspace_timeout_is_reported():
+    """The reverse passes report bounded-wait timeouts in the adjoint
+    workspace's own header word, read by sles_adjoint_check."""
+    from sles.adjoint import RK4Rollout
+    ro = RK4Rollout(32, 1e-3, 1e-3, les="Smagorinsky", Cs=0.17, dtype=torch.float32)
+    assert ro.plan.adjoint_check(ro._ws) == 0
+    L = nat.load_library()
+    assert L.sles_selftest_wait_timeout_word(ctypes.c_void_p(ro._ws), nat.stream_handle(ro.device)) == 0
+    with pytest.raises(nat.SlesError) as e:
+        ro.plan.adjoint_check(ro._ws)
+    assert e.value.status == 5  # SLES_ERR_TIMEOUT
+    assert ro.plan.adjoint_check(ro._ws) == 0  # cleared
+    assert ro.plan.check() == 0  # the forward plan's word is separate

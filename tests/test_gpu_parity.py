@@ -12,13 +12,13 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import GOLDEN
+from conftest import GOLDEN, step_cases
 from sles import ETD2_method, RK3_method, RK4_method
 from sles.initial import initial_velocity, initial_vorticity
 from sles.initialize_domain import InitializeDomain
 
 pytestmark = pytest.mark.gpu
-CASES = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f != "ops16.npz")
+CASES = step_cases()
 STEP = {"RK4": RK4_method, "RK3": RK3_method, "ETD2": ETD2_method}
 
 

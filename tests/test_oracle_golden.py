@@ -12,10 +12,10 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+from conftest import GOLDEN, solver_cases, step_cases
 from oracle import spectral_oracle as so
 
-CASES = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f != "ops16.npz")
+CASES = step_cases()
 
 
 def rel(a, b):
@@ -112,3 +112,46 @@ def test_etd2_corrected_coefficients_limit():
     z = 1e-4 * 1e-3 * 10**6
     c1x = 1e-3 * ((1 - z) * np.exp(-z) - 1 + 2 * z) / z**2
     assert c1[-1] == pytest.approx(c1x, rel=1e-12)
+
+
+def _oracle_from_solver_meta(meta):
+    return so.OracleDomain.from_reference_args(
+        meta["No_of_gridpoint"], dimension=meta["dimension"], nu=meta["nu"], LES_ON=meta.get("LES_ON", 0),
+        LES_model=meta.get("LES_model"), Cs=meta.get("Cs", 0.14), method=meta["method"], parity=True)
+
+
+@pytest.mark.parametrize("name", solver_cases())
+def test_oracle_driver_loop_matches_reference(name):
+    """The oracle's restatement of spectralMethodSolver (adaptive dt, E(k)
+    snapshots) against the reference's own run of it."""
+    z, meta = load(name)
+    d = _oracle_from_solver_meta(meta)
+    if "omega0" in z:
+        so.initial_vorticity(d, z["omega0"])
+    else:
+        so.initial_velocity(d, *z["u0"])
+    steps, dts, umaxs, snaps = so.solver_loop(d, meta["final_time"], CFL=meta["CFL"], No_Ek_plot=meta["No_Ek_plot"])
+    assert steps == meta["steps"]
+    np.testing.assert_allclose(dts, z["dt_seq"], rtol=1e-12)
+    np.testing.assert_allclose(umaxs, z["umax_seq"], rtol=1e-12)
+    assert rel(d.U_hat, z["U_hat_final"]) < 1e-11
+    cols = json.loads(str(z["ek_columns"]))
+    assert cols == [c for t, _, _ in snaps for c in ("k-%g" % t, "Ek-%g" % t)]
+    vals = np.concatenate([np.stack([tk, tE], 1) for _, tk, tE in snaps], 1)
+    np.testing.assert_allclose(vals, z["ek_values"], rtol=1e-11, atol=0)
+
+
+def test_oracle_diagnostics_match_reference():
+    z = np.load(os.path.join(GOLDEN, "diag16.npz"))
+    for tag in ("rand16", "noise16", "vort32"):
+        meta = json.loads(str(z[tag + "_meta"]))
+        d = so.OracleDomain(meta["N"], meta["dimension"], nu=meta["nu"])
+        if tag + "_omega0" in z:
+            so.initial_vorticity(d, z[tag + "_omega0"])
+        else:
+            so.initial_velocity(d, *z[tag + "_u0"])
+        assert so.U_square(d) == pytest.approx(float(z[tag + "_U_square"]), rel=1e-13)
+        assert so.dissipation_rate(d) == pytest.approx(float(z[tag + "_dissipation_rate"]), rel=1e-12)
+        tk, tE = so.reference_binned_spectrum(d)
+        np.testing.assert_allclose(tk, z[tag + "_temp_k"], rtol=1e-14)
+        np.testing.assert_allclose(tE, z[tag + "_temp_Ek"], rtol=1e-12)
