@@ -733,7 +733,7 @@ def main():
     ap.add_argument("--precision", default="float32", choices=["float32", "float64"])
     ap.add_argument("--xvar", type=int, default=-1, help="x-pass variant of --only steps (-1: default/cached)")
     args = ap.parse_args()
-    assert args.warmup >= 3 or args.impl == "reference", "at least 3 warm-up steps"
+    assert args.warmup >= 3 or args.impl == "reference" or args.only, "at least 3 warm-up steps"
     global TUNE
     TUNE = not args.no_tune
 

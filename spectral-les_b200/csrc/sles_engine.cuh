@@ -13,6 +13,7 @@
 #include "sles_misc.cuh"
 #include "sles_passes.cuh"
 #include "sles_rhs.cuh"
+#include "sles_xtma.cuh"
 #include "sles_adjoint.cuh"
 
 namespace sles {
@@ -141,6 +142,22 @@ inline int make_tmap(CUtensorMap* m, const void* base, int epc, int nk, long lon
   cuuint64_t dims[4] = {(cuuint64_t)nk * epc, (cuuint64_t)rows, (cuuint64_t)slices, (cuuint64_t)nslot};
   cuuint64_t strides[3] = {(cuuint64_t)row_stride_b, (cuuint64_t)slice_stride_b, (cuuint64_t)slot_stride_b};
   cuuint32_t box[4] = {(cuuint32_t)(box_cols * epc), (cuuint32_t)box_rows, 1, 1};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(base), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? SLES_OK : SLES_ERR_CUDA;
+}
+
+// the same map with box {box_cols*epc, box1, box2, 1}
+inline int make_tmap_box(CUtensorMap* m, const void* base, int epc, int nk, long long rows, long long row_stride_b,
+                         long long slices, long long slice_stride_b, long long nslot, long long slot_stride_b,
+                         int box_cols, int box1, int box2) {
+  PFN_cuTensorMapEncodeTiled_v12000 fn = tmap_encoder();
+  if (!fn) return SLES_ERR_CUDA;
+  cuuint64_t dims[4] = {(cuuint64_t)nk * epc, (cuuint64_t)rows, (cuuint64_t)slices, (cuuint64_t)nslot};
+  cuuint64_t strides[3] = {(cuuint64_t)row_stride_b, (cuuint64_t)slice_stride_b, (cuuint64_t)slot_stride_b};
+  cuuint32_t box[4] = {(cuuint32_t)(box_cols * epc), (cuuint32_t)box1, (cuuint32_t)box2, 1};
   cuuint32_t es[4] = {1, 1, 1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(base), dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -351,15 +368,13 @@ struct EngineImpl final : Engine {
     switch (p.xvar) {
       case 1: return xpass_v<LES, PAR2D, 1>(p, a, st);
       case 2: return xpass_v<LES, PAR2D, 2>(p, a, st);
+      case 3: return xpass_tma<LES, PAR2D>(p, a, st);
       default: return xpass_v<LES, PAR2D, 0>(p, a, st);
     }
   }
-  template <int LES, int PAR2D, int XV>
-  int xpass_v(const PlanInfo& p, XArgs<Tp> a, cudaStream_t st) {
-    using K = XGeo<Tp, N, FXV<XV>, DIM, XV>;
-    a.nchunks = xchunks<XV>(p);
-    // state tiles the stage reads (ucur for viscous/forcing/update; u0 when
-    // distinct from ucur; u1 = RK4 accumulator or ETD2's previous F1)
+  // state tiles a stage reads (u_cur for viscous/forcing/update; u0 when
+  // distinct from u_cur; u1 = RK4 accumulator or ETD2's previous F1)
+  static void set_needs(XArgs<Tp>& a) {
     a.need_uc = a.need_u0 = a.need_u1 = 0;
     if (a.fwd && a.kind != KX_RAW) {
       a.need_uc = 1;
@@ -367,6 +382,47 @@ struct EngineImpl final : Engine {
       a.need_u0 = (uses_u0 && a.u0 != a.ucur) ? 1 : 0;
       a.need_u1 = (a.kind == KX_RK4 || a.kind == KX_ETD2P || a.kind == KX_ETD2C) ? 1 : 0;
     }
+  }
+  // x-pass variant XV_TMA (sles_xtma.cuh): compiled for the 3D grids 128, 256
+  // and 512; elsewhere the variant runs as variant 0
+  static constexpr bool HAS_XTMA = DIM == 3 && (N == 128 || N == 256 || N == 512);
+  template <int LES, int PAR2D>
+  int xpass_tma(const PlanInfo& p, XArgs<Tp> a, cudaStream_t st) {
+    if constexpr (!HAS_XTMA) {
+      return xpass_v<LES, PAR2D, 0>(p, a, st);
+    } else {
+      using F = typename WithPad<typename PlanLo<Tp, N>::F, SLES_X_PADD>::F;
+      using K = XTGeo<Tp, N, F>;
+      XTArgs<Tp> P{};
+      a.nchunks = (p.nk + K::W - 1) / K::W;
+      set_needs(a);
+      a.err = p.flags;
+      P.a = a;
+      const long long cb = sizeof(C), row = (long long)p.nkp * cb, slice = (long long)N * p.nkp * cb;
+      const long long fsb = p.hc_elems * cb;
+      // {columns, ky rows, x slices, slots}; box {W columns, 1 ky row, RB x rows, 1 slot}
+      auto mk = [&](CUtensorMap* m, const void* base, long long nslot) {
+        return make_tmap_box(m, base, K::EPC, p.nk, N, row, N, slice, nslot, fsb, K::W, 1, K::RB);
+      };
+      SLES_TRY(mk(&P.tws, slot(p, 0), p.ws_fields));
+      const void* cur = a.fwd ? (const void*)a.ucur : (const void*)a.uinv;
+      SLES_TRY(mk(&P.tcur, cur ? cur : slot(p, 0), 3));
+      SLES_TRY(mk(&P.t0, a.need_u0 ? (const void*)a.u0 : slot(p, 0), 3));
+      SLES_TRY(mk(&P.t1, a.need_u1 ? (const void*)a.u1 : slot(p, 0), 3));
+      const long long items = (long long)N * a.nchunks;
+      if (a.kind == KX_ETD2P || a.kind == KX_ETD2C) {
+        if (LES) return launch_persistent(k_xpass_tma<Tp, N, F, 1, 1>, items, K::THREADS, K::SMEM, st, P);
+        return launch_persistent(k_xpass_tma<Tp, N, F, 0, 1>, items, K::THREADS, K::SMEM, st, P);
+      }
+      if (LES) return launch_persistent(k_xpass_tma<Tp, N, F, 1, 0>, items, K::THREADS, K::SMEM, st, P);
+      return launch_persistent(k_xpass_tma<Tp, N, F, 0, 0>, items, K::THREADS, K::SMEM, st, P);
+    }
+  }
+  template <int LES, int PAR2D, int XV>
+  int xpass_v(const PlanInfo& p, XArgs<Tp> a, cudaStream_t st) {
+    using K = XGeo<Tp, N, FXV<XV>, DIM, XV>;
+    a.nchunks = xchunks<XV>(p);
+    set_needs(a);
     a.err = p.flags;
     const long long items = (long long)(DIM == 3 ? N : 1) * a.nchunks;
     if (a.kind == KX_ETD2P || a.kind == KX_ETD2C)

@@ -239,8 +239,9 @@ struct TGeo {
 //      ring of 2 buffers with per-thread cp.async, 8 warps per SM
 //   2: W = 32-byte rows, the same ring, 12 warps per SM
 // A ring that does not fit the variant's shared-memory budget falls back to
-// direct loads (NB = 0).
-constexpr int X_VARIANTS = 3;
+// direct loads (NB = 0).  Variant 3 (sles_xtma.cuh) streams every tile through
+// a TMA ring and keeps the projected components in registers.
+constexpr int X_VARIANTS = 4;
 template <typename Tp, int N, class F, int DIM, int XV>
 struct XGeo {
   using C = typename CT<Tp>::C;

@@ -1,7 +1,9 @@
 """Kernel variants and the autotuner: every x-pass variant gives the same
-states (bit-identical in the float32 cases here; float64 up to the compiler's
-floating-point contraction, 1e-14 relative); tune() picks one, records it and
-new domains pick it up."""
+states (float32: variants 0-2 bit-identical, the TMA-ring variant 3 within
+1e-6 relative, the compiler being free to contract a*b+c differently in it;
+float64 up to contraction, 1e-14 relative); tune() picks one, records it and
+new domains pick it up.  Variant 3 is compiled for the 3D grids 128, 256 and
+512 (elsewhere it runs variant 0)."""
 import json
 
 import pytest
@@ -24,7 +26,14 @@ CASES = [  # (dim, n, dtype, les, method, parity)
     (3, 48, "float64", "Smagorinsky", "RK4", True),
     (3, 64, "float32", None, "RK4", True),
     (2, 256, "float32", None, "RK4", True),
+    (3, 128, "float32", "Smagorinsky", "RK3", True),
+    (3, 128, "float64", "vreman", "RK4", True),
+    (3, 128, "float32", None, "RK4", True),
+    (3, 128, "float64", "Smagorinsky", "ETD2", True),
+    (3, 256, "float32", "Smagorinsky", "RK3", True),
+    (3, 256, "float32", "Smagorinsky", "RK3", False),
 ]
+NV = 4
 
 
 def _dom(dim, n, dtype, les, method, parity):
@@ -42,17 +51,22 @@ def _dom(dim, n, dtype, les, method, parity):
 @pytest.mark.parametrize("case", CASES, ids=lambda c: "%dd%d_%s_%s_%s" % (c[0], c[1], c[2], c[3], c[4]))
 def test_variants_are_bit_identical(case):
     ref = None
-    for v in range(3):
+    for v in range(NV):
         d = _dom(*case)
-        assert d._plan.variant_count(nat.PASS_X) == 3
+        assert d._plan.variant_count(nat.PASS_X) == NV
         d._plan.set_variant(v, nat.PASS_X)
         for _ in range(3):
             STEP[case[4]](d)
+        d._plan.check()
         u = d.U_hat.clone()
+        del d
         if ref is None:
             ref = u
-        elif case[2] == "float32":
+        elif case[2] == "float32" and v < 3:
             assert torch.equal(u, ref), "x-pass variant %d differs" % v
+        elif case[2] == "float32":
+            rel = float(torch.linalg.vector_norm(u - ref) / torch.linalg.vector_norm(ref))
+            assert rel < 1e-6, "x-pass variant %d differs by %g" % (v, rel)
         else:
             rel = float(torch.linalg.vector_norm(u - ref) / torch.linalg.vector_norm(ref))
             assert rel < 1e-14, "x-pass variant %d differs by %g" % (v, rel)
@@ -63,7 +77,7 @@ def test_tune_records_and_reapplies(tmp_path, monkeypatch):
     d = _dom(3, 64, "float32", "Smagorinsky", "RK3", True)
     before = d.U_hat.clone()
     times = autotune.tune(d, steps=2, repeats=2)
-    assert set(times) == {0, 1, 2} and all(t > 0 for t in times.values())
+    assert set(times) == set(range(NV)) and all(t > 0 for t in times.values())
     win = min(times, key=times.get)
     assert d._plan.get_variant(nat.PASS_X) == win
     assert torch.equal(d.U_hat, before)  # tuning does not advance the domain

@@ -152,7 +152,8 @@ def test_diagnostics_match_reference():
         assert diagnostics.dissipation_rate(d) == pytest.approx(float(z[tag + "_dissipation_rate"]), rel=1e-12)
         tk, tE = diagnostics.reference_binned_spectrum(d)
         np.testing.assert_allclose(tk, z[tag + "_temp_k"], rtol=1e-13)
-        np.testing.assert_allclose(tE, z[tag + "_temp_Ek"], rtol=1e-12)
+        # bins beyond the field's band hold round-off-level energy: an absolute floor
+        np.testing.assert_allclose(tE, z[tag + "_temp_Ek"], rtol=1e-12, atol=1e-14 * np.max(z[tag + "_temp_Ek"]))
 
 
 @pytest.mark.parametrize("dim,n", [(3, 16), (3, 32), (2, 64)])
