@@ -93,6 +93,53 @@ enum { SLES_PASS_X = 0 };
 int sles_plan_variant_count(const sles_plan* plan, int pass);
 int sles_plan_get_variant(const sles_plan* plan, int pass);
 int sles_plan_set_variant(sles_plan* plan, int pass, int variant);
+/*
+ * Slab decomposition of one 3D domain over P ranks (one GPU each), the
+ * layout of the reference's mpi4py-fft PFFT (src/initialize_domain.py:59-65,
+ * slab bounds src/utilites.py:18-24 with N divisible by P): rank r holds the
+ * ky rows [r m, (r+1) m) of every spectral field, as [N kx][m ky][nkp], and the
+ * x planes [r m, (r+1) m) of physical space (m = N/P <= 256).  Call
+ * sles_plan_set_slab before sles_plan_set_workspace; afterwards
+ * sles_plan_layout reports the slab's element counts, the whole-grid entry
+ * points (sles_rhs, sles_stage, transforms, diagnostics, adjoint, static
+ * workspace) return SLES_ERR_STATE, and one RHS evaluation is
+ *   sles_slab_prime   (or the previous sles_slab_stage): the inverse
+ *                     x-transforms of the state on this rank's ky rows, into
+ *                     the n_exchange1 fields at send1
+ *   exchange 1        the caller's all-to-all (NCCL): for each field f, block
+ *                     q (block_elems elements) of send1[f] goes to rank q and
+ *                     block r of recv1[f] on rank q comes from rank r
+ *                     (src/initialize_domain.py:59-65: the PFFT global transpose)
+ *   sles_slab_middle  y inverse (reading recv1 across the P blocks), the fused
+ *                     z pass (u x omega, eddy viscosity, stress), y forward,
+ *                     whose n_exchange2 output fields are stored at send2 as P
+ *                     blocks; umax_bits (optional device word, zeroed by the
+ *                     caller) receives the ordered encoding of this rank's
+ *                     max u (find_max_velocity, src/SM_solver.py:245-255; the
+ *                     caller all-reduces the max over ranks)
+ *   exchange 2        the same all-to-all from send2 into recv2
+ *   sles_slab_stage   x forward, combine, projection, the stage update
+ *                     (as sles_stage; not SLES_STAGE_RECORD_F1/PRIMED, not the
+ *                     reference's ETD2 with LES), and unless
+ *                     SLES_STAGE_NO_PREPARE the priming of the next evaluation.
+ * State fields (u_cur, u0, u1, u_out, aux) are 3 fields in the slab layout.
+ * The exchange buffers live in the plan's workspace (sles_slab_buffers).
+ */
+typedef struct sles_slab_layout {
+  int32_t nranks, rank, m;        /* P, r, rows per block (N/P) */
+  int32_t n_exchange1;            /* fields of exchange 1 (6 with LES, else 5) */
+  int32_t n_exchange2;            /* fields of exchange 2 (6 with LES, else 3) */
+  int32_t reserved;
+  int64_t block_elems;            /* complex elements per block: m*m*nkp */
+  int64_t field_elems;            /* complex elements per field on this rank: N*m*nkp */
+} sles_slab_layout;
+int sles_plan_set_slab(sles_plan* plan, int nranks, int rank);
+int sles_slab_info(const sles_plan* plan, sles_slab_layout* out);
+int sles_slab_buffers(sles_plan* plan, void** send1, void** recv1, void** send2, void** recv2);
+int sles_slab_prime(sles_plan* plan, const void* u_state, void* stream);
+int sles_slab_middle(sles_plan* plan, unsigned long long* umax_bits, void* stream);
+int sles_slab_stage(sles_plan* plan, int stage, double dt, const void* u_cur, const void* u0, void* u1,
+                    void* u_out, void* aux_out, int flags, void* stream);
 /* Bytes of device workspace the plan needs for intermediate fields. */
 size_t sles_plan_workspace_bytes(const sles_plan* plan);
 /* Attach caller-owned device workspace (>= sles_plan_workspace_bytes). */

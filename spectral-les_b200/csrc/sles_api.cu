@@ -81,7 +81,45 @@ int sles_plan_create(const sles_plan_desc* d, sles_plan** out) {
   I.flags = nullptr;
   I.scal = nullptr;
   I.xvar = eng->default_xvar();
+  I.slab_p = 1;
+  I.slab_r = 0;
+  I.slab_m = d->n;
+  I.slab_n1 = I.slab_n2 = 0;
   *out = p;
+  return SLES_OK;
+}
+
+int sles_plan_set_slab(sles_plan* p, int nranks, int rank) {
+  if (!p) return SLES_ERR_INVALID_ARG;
+  sles::PlanInfo& I = p->info;
+  if (I.ws) return SLES_ERR_STATE;  // the layout must be fixed before the workspace is attached
+  if (I.d.dim != 3) return SLES_ERR_UNSUPPORTED;
+  if (nranks < 1 || rank < 0 || rank >= nranks || I.d.n % nranks != 0) return SLES_ERR_INVALID_ARG;
+  const int m = I.d.n / nranks;
+  if (m > 256) return SLES_ERR_UNSUPPORTED;  // a line's P blocks of m rows arrive as one TMA box
+  int n1 = 0, n2 = 0;
+  if (int s = p->eng->slab_counts(I, &n1, &n2)) return s;
+  I.slab_p = nranks;
+  I.slab_r = rank;
+  I.slab_m = m;
+  I.slab_n1 = n1;
+  I.slab_n2 = n2;
+  I.hc_elems = (long long)I.d.n * m * I.nkp;
+  I.real_elems = (long long)m * I.d.n * I.d.n;
+  I.ws_fields = p->eng->ws_fields_needed(I) + n1 + n2;
+  return SLES_OK;
+}
+
+int sles_slab_info(const sles_plan* p, sles_slab_layout* out) {
+  if (!p || !out) return SLES_ERR_INVALID_ARG;
+  const sles::PlanInfo& I = p->info;
+  out->nranks = I.slab_p;
+  out->rank = I.slab_r;
+  out->m = I.slab_m;
+  out->n_exchange1 = I.slab_n1;
+  out->n_exchange2 = I.slab_n2;
+  out->block_elems = (int64_t)I.slab_m * I.slab_m * I.nkp;
+  out->field_elems = I.hc_elems;
   return SLES_OK;
 }
 
@@ -149,32 +187,39 @@ static int ready(sles_plan* p) {
   return SLES_OK;
 }
 
-int sles_fft_r2c(sles_plan* p, const void* in, void* out, int nf, void* stream) {
+// entry points that work on the whole grid: not on a plan set to a slab
+static int ready_full(sles_plan* p) {
   if (int s = ready(p)) return s;
+  if (p->info.slab_n1 != 0) return SLES_ERR_STATE;
+  return SLES_OK;
+}
+
+int sles_fft_r2c(sles_plan* p, const void* in, void* out, int nf, void* stream) {
+  if (int s = ready_full(p)) return s;
   if (!in || !out || nf < 0) return SLES_ERR_INVALID_ARG;
   return p->eng->fft_r2c(p->info, in, out, nf, (cudaStream_t)stream);
 }
 
 int sles_fft_c2r(sles_plan* p, const void* in, void* out, int nf, void* stream) {
-  if (int s = ready(p)) return s;
+  if (int s = ready_full(p)) return s;
   if (!in || !out || nf < 0) return SLES_ERR_INVALID_ARG;
   return p->eng->fft_c2r(p->info, in, out, nf, (cudaStream_t)stream);
 }
 
 int sles_velocity_curl(sles_plan* p, const void* uh, void* u, void* curl, void* stream) {
-  if (int s = ready(p)) return s;
+  if (int s = ready_full(p)) return s;
   if (!uh) return SLES_ERR_INVALID_ARG;
   return p->eng->velocity_curl(p->info, uh, u, curl, (cudaStream_t)stream);
 }
 
 int sles_velocity_gradient(sles_plan* p, const void* uh, void* grad, void* stream) {
-  if (int s = ready(p)) return s;
+  if (int s = ready_full(p)) return s;
   if (!uh || !grad) return SLES_ERR_INVALID_ARG;
   return p->eng->velocity_gradient(p->info, uh, grad, (cudaStream_t)stream);
 }
 
 int sles_rhs(sles_plan* p, const void* uh, const void* uphys, const void* cphys, void* du, void* f1, void* stream) {
-  if (int s = ready(p)) return s;
+  if (int s = ready_full(p)) return s;
   if (!uh || !du) return SLES_ERR_INVALID_ARG;
   if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
   return p->eng->rhs(p->info, uh, uphys, cphys, du, f1, (cudaStream_t)stream);
@@ -182,7 +227,7 @@ int sles_rhs(sles_plan* p, const void* uh, const void* uphys, const void* cphys,
 
 int sles_stage(sles_plan* p, int stage, double dt, const void* ucur, const void* u0, void* u1, void* uout, void* aux,
                const void* uphys, const void* cphys, int flags, void* stream) {
-  if (int s = ready(p)) return s;
+  if (int s = ready_full(p)) return s;
   if (!ucur || !uout || !(dt == dt)) return SLES_ERR_INVALID_ARG;
   if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
   const int scheme = (flags & sles::STAGE_RK4) ? SLES_RK4 : p->info.d.scheme;
@@ -192,7 +237,7 @@ int sles_stage(sles_plan* p, int stage, double dt, const void* ucur, const void*
 
 int sles_stage_ctl(sles_plan* p, int stage, void* dtctl, int parity, const void* ucur, const void* u0, void* u1,
                    void* uout, void* aux, const void* uphys, const void* cphys, int flags, void* stream) {
-  if (int s = ready(p)) return s;
+  if (int s = ready_full(p)) return s;
   if (!dtctl || !ucur || !uout || (parity != 0 && parity != 1)) return SLES_ERR_INVALID_ARG;
   if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
   const int scheme = (flags & sles::STAGE_RK4) ? SLES_RK4 : p->info.d.scheme;
@@ -230,6 +275,45 @@ int sles_selftest_wait_timeout(sles_plan* p, void* stream) {
   return sles::launch(sles::k_wait_selftest, 1, 32, 0, (cudaStream_t)stream, p->info.flags, 4096L);
 }
 
+static int slab_ready(sles_plan* p) {
+  if (int s = ready(p)) return s;  // (a slab plan is never ready_full)
+  if (p->info.slab_n1 == 0) return SLES_ERR_STATE;  // sles_plan_set_slab was not called
+  return SLES_OK;
+}
+
+int sles_slab_buffers(sles_plan* p, void** send1, void** recv1, void** send2, void** recv2) {
+  if (int s = slab_ready(p)) return s;
+  const sles::PlanInfo& I = p->info;
+  char* slots = reinterpret_cast<char*>(I.ws) + sles::slots_offset(I.d.dim, I.d.n);
+  const size_t fb = (size_t)I.hc_elems * I.elem_bytes;
+  const int base = I.ws_fields - I.slab_n1 - I.slab_n2;
+  if (send1) *send1 = slots;
+  if (recv2) *recv2 = slots;
+  if (recv1) *recv1 = slots + (size_t)base * fb;
+  if (send2) *send2 = slots + (size_t)(base + I.slab_n1) * fb;
+  return SLES_OK;
+}
+
+int sles_slab_prime(sles_plan* p, const void* u_state, void* stream) {
+  if (int s = slab_ready(p)) return s;
+  if (!u_state) return SLES_ERR_INVALID_ARG;
+  return p->eng->slab_prime(p->info, u_state, (cudaStream_t)stream);
+}
+
+int sles_slab_middle(sles_plan* p, unsigned long long* umax_bits, void* stream) {
+  if (int s = slab_ready(p)) return s;
+  return p->eng->slab_middle(p->info, umax_bits, (cudaStream_t)stream);
+}
+
+int sles_slab_stage(sles_plan* p, int stage, double dt, const void* ucur, const void* u0, void* u1, void* uout,
+                    void* aux, int flags, void* stream) {
+  if (int s = slab_ready(p)) return s;
+  if (!ucur || !uout || !(dt == dt)) return SLES_ERR_INVALID_ARG;
+  const int scheme = (flags & sles::STAGE_RK4) ? SLES_RK4 : p->info.d.scheme;
+  if ((scheme == SLES_RK4 && (!u0 || !u1)) || (scheme == SLES_RK3 && !u0)) return SLES_ERR_INVALID_ARG;
+  return p->eng->slab_stage(p->info, stage, dt, ucur, u0, u1, uout, aux, flags, (cudaStream_t)stream);
+}
+
 int sles_selftest_wait_timeout_word(void* word, void* stream) {
   if (!word || ((uintptr_t)word) % sizeof(unsigned) != 0) return SLES_ERR_INVALID_ARG;
   return sles::launch(sles::k_wait_selftest, 1, 32, 0, (cudaStream_t)stream, reinterpret_cast<unsigned*>(word),
@@ -238,13 +322,13 @@ int sles_selftest_wait_timeout_word(void* word, void* stream) {
 
 int sles_diag(sles_plan* p, const void* uh, const void* uphys, double* out, double* spectrum, int nshell,
               void* stream) {
-  if (int s = ready(p)) return s;
+  if (int s = ready_full(p)) return s;
   if (!uh || !out || nshell < 0) return SLES_ERR_INVALID_ARG;
   return p->eng->diag(p->info, uh, uphys, out, spectrum, nshell, (cudaStream_t)stream);
 }
 
 int sles_profile_rhs(sles_plan* p, const void* uh, void* du, int iters, double* ms, void* stream) {
-  if (int s = ready(p)) return s;
+  if (int s = ready_full(p)) return s;
   if (!uh || !du || !ms || iters < 1) return SLES_ERR_INVALID_ARG;
   return p->eng->profile_rhs(p->info, uh, du, iters, ms, (cudaStream_t)stream);
 }
@@ -259,6 +343,7 @@ size_t sles_adjoint_workspace_bytes(const sles_plan* p) {
 static int adjoint_info(sles_plan* p, void* adj_ws, sles::PlanInfo* out) {
   if (!p || !adj_ws) return SLES_ERR_INVALID_ARG;
   if (p->info.d.dim != 3) return SLES_ERR_UNSUPPORTED;
+  if (p->info.slab_n1 != 0) return SLES_ERR_STATE;
   if (((uintptr_t)adj_ws) % 256 != 0) return SLES_ERR_INVALID_ARG;
   *out = p->info;
   out->ws = adj_ws;
@@ -368,6 +453,7 @@ int static_ws_address(void** out) {
 extern "C" int sles_rhs_static_workspace(sles_plan* p, const void* uh, const void* uphys, const void* cphys,
                                          void* du, void* f1, void* stream) {
   if (!p || !uh || !du) return SLES_ERR_INVALID_ARG;
+  if (p->info.slab_n1 != 0) return SLES_ERR_STATE;
   if (sles_plan_workspace_bytes(p) > (size_t)SLES_STATIC_WORKSPACE_BYTES) return SLES_ERR_WORKSPACE;
   if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
   void* ws = nullptr;

@@ -29,6 +29,11 @@ struct PlanInfo {
   unsigned* flags;       // device error word inside the workspace
   double* scal;          // device scalar scratch inside the workspace (64 doubles)
   int xvar;              // x-pass variant (XGeo), set by default or by the autotuner
+  // slab decomposition over P ranks (3D): this rank holds ky rows [r*m, (r+1)*m)
+  // of spectral fields and x planes [r*m, (r+1)*m) of physical ones (m = N/P);
+  // P = 1, m = N: the whole grid
+  int slab_p, slab_r, slab_m;
+  int slab_n1, slab_n2;  // fields of the two exchanges (x-inverse outputs, y-forward outputs)
 };
 
 // workspace header: error word + scalar scratch, then the diagnostics area,
@@ -62,6 +67,13 @@ struct Engine {
   virtual int adjoint_prime(PlanInfo& pa, const void* u_state, const void* lam, cudaStream_t st) = 0;
   virtual int adjoint_stage(PlanInfo& pa, int s, double dt, const void* unext, void* ubar, void* acc, void* lam,
                             double* csgrad, cudaStream_t st) = 0;
+  // slab decomposition (3D): exchange field counts, and the three pass groups
+  // around the two exchanges of one RHS evaluation
+  virtual int slab_counts(const PlanInfo& p, int* n1, int* n2) const = 0;
+  virtual int slab_prime(PlanInfo& p, const void* u, cudaStream_t st) = 0;
+  virtual int slab_middle(PlanInfo& p, unsigned long long* umax, cudaStream_t st) = 0;
+  virtual int slab_stage(PlanInfo& p, int stage, double dt, const void* ucur, const void* u0, void* u1, void* uout,
+                         void* aux, int flags, cudaStream_t st) = 0;
 };
 
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? SLES_OK : SLES_ERR_CUDA; }
@@ -160,6 +172,25 @@ inline int make_tmap_box(CUtensorMap* m, const void* base, int epc, int nk, long
   cuuint32_t box[4] = {(cuuint32_t)(box_cols * epc), (cuuint32_t)box1, (cuuint32_t)box2, 1};
   cuuint32_t es[4] = {1, 1, 1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(base), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? SLES_OK : SLES_ERR_CUDA;
+}
+
+// 5D map over a slab exchange buffer [fields][P blocks][m x planes][m rows][nkp]:
+// dims {nk*epc, m rows, m planes, P blocks, fields}; box {box_cols*epc, m, 1, P, 1}
+// (one whole line of N = P*m rows, landing as [P][m][cols] = [rows][cols])
+inline int make_tmap_split(CUtensorMap* mp, const void* base, int epc, int nk, int nkp, long long m, long long P,
+                           long long nfields, long long field_stride_b, int elem_b, int box_cols) {
+  PFN_cuTensorMapEncodeTiled_v12000 fn = tmap_encoder();
+  if (!fn) return SLES_ERR_CUDA;
+  const long long row_b = (long long)nkp * elem_b;
+  cuuint64_t dims[5] = {(cuuint64_t)nk * epc, (cuuint64_t)m, (cuuint64_t)m, (cuuint64_t)P, (cuuint64_t)nfields};
+  cuuint64_t strides[4] = {(cuuint64_t)row_b, (cuuint64_t)(m * row_b), (cuuint64_t)(m * m * row_b),
+                           (cuuint64_t)field_stride_b};
+  cuuint32_t box[5] = {(cuuint32_t)(box_cols * epc), (cuuint32_t)m, 1, (cuuint32_t)P, 1};
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = fn(mp, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<void*>(base), dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? SLES_OK : SLES_ERR_CUDA;
@@ -360,6 +391,8 @@ struct EngineImpl final : Engine {
     a.forcing = (Tp)p.d.forcing;
     a.kmax = 2.0 / 3.0 * (double)(N / 2 + 1);  // initialize_domain.py:79
     a.nu_d = p.d.nu;
+    a.nsl = p.slab_m;
+    a.ky0 = p.slab_r * p.slab_m;
     return a;
   }
 
@@ -398,18 +431,18 @@ struct EngineImpl final : Engine {
       set_needs(a);
       a.err = p.flags;
       P.a = a;
-      const long long cb = sizeof(C), row = (long long)p.nkp * cb, slice = (long long)N * p.nkp * cb;
+      const long long cb = sizeof(C), row = (long long)p.nkp * cb, slice = (long long)a.nsl * p.nkp * cb;
       const long long fsb = p.hc_elems * cb;
       // {columns, ky rows, x slices, slots}; box {W columns, 1 ky row, RB x rows, 1 slot}
       auto mk = [&](CUtensorMap* m, const void* base, long long nslot) {
-        return make_tmap_box(m, base, K::EPC, p.nk, N, row, N, slice, nslot, fsb, K::W, 1, K::RB);
+        return make_tmap_box(m, base, K::EPC, p.nk, a.nsl, row, N, slice, nslot, fsb, K::W, 1, K::RB);
       };
       SLES_TRY(mk(&P.tws, slot(p, 0), p.ws_fields));
       const void* cur = a.fwd ? (const void*)a.ucur : (const void*)a.uinv;
       SLES_TRY(mk(&P.tcur, cur ? cur : slot(p, 0), 3));
       SLES_TRY(mk(&P.t0, a.need_u0 ? (const void*)a.u0 : slot(p, 0), 3));
       SLES_TRY(mk(&P.t1, a.need_u1 ? (const void*)a.u1 : slot(p, 0), 3));
-      const long long items = (long long)N * a.nchunks;
+      const long long items = (long long)a.nsl * a.nchunks;
       if (a.kind == KX_ETD2P || a.kind == KX_ETD2C) {
         if (LES) return launch_persistent(k_xpass_tma<Tp, N, F, 1, 1>, items, K::THREADS, K::SMEM, st, P);
         return launch_persistent(k_xpass_tma<Tp, N, F, 0, 1>, items, K::THREADS, K::SMEM, st, P);
@@ -424,7 +457,7 @@ struct EngineImpl final : Engine {
     a.nchunks = xchunks<XV>(p);
     set_needs(a);
     a.err = p.flags;
-    const long long items = (long long)(DIM == 3 ? N : 1) * a.nchunks;
+    const long long items = (long long)(DIM == 3 ? a.nsl : 1) * a.nchunks;
     if (a.kind == KX_ETD2P || a.kind == KX_ETD2C)
       return launch_persistent(k_xpass<Tp, N, FXV<XV>, DIM, LES, PAR2D, 1, XV>, items, K::THREADS, K::SMEM, st, a);
     return launch_persistent(k_xpass<Tp, N, FXV<XV>, DIM, LES, PAR2D, 0, XV>, items, K::THREADS, K::SMEM, st, a);
@@ -435,22 +468,41 @@ struct EngineImpl final : Engine {
     return xpass<1, 0>(p, a, st);
   }
 
+  // slab exchange buffers inside the workspace (after the pass slots): the
+  // x-inverse outputs go out from slots [0, n1) and arrive in `recv1`; the
+  // y-forward outputs go out from `send2` and arrive in slots [0, n2)
+  static int pass_slots(const PlanInfo& p) { return p.ws_fields - p.slab_n1 - p.slab_n2; }
+  static C* slab_recv1(const PlanInfo& p) { return slot(p, pass_slots(p)); }
+  static C* slab_send2(const PlanInfo& p) { return slot(p, pass_slots(p) + p.slab_n1); }
+
+  // split: on a slab (P > 1 or an explicit exchange), the inverse pass reads the
+  // exchange buffer and the forward pass stores into the outgoing one
   template <int LES>
-  int ypass(const PlanInfo& p, int inv, cudaStream_t st) {
+  int ypass(const PlanInfo& p, int inv, cudaStream_t st, bool split = false) {
     if (DIM != 3) return SLES_OK;
     using K = YGeoI<LES>;  // tile geometry (the tensor map) is the same for the forward plan
     using KF = YGeoF<LES>;
     YArgs<Tp> a{};
     const long long cb = sizeof(C);
-    SLES_TRY(make_tmap(&a.tm, slot(p, 0), K::EPC, p.nk, N, (long long)p.nkp * cb, N, (long long)N * p.nkp * cb,
-                       p.ws_fields, p.hc_elems * cb, K::W, K::RB));
+    const int M = p.slab_m;
+    if (split && inv) {
+      SLES_TRY(make_tmap_split(&a.tm, slab_recv1(p), K::EPC, p.nk, p.nkp, M, p.slab_p, p.slab_n1, p.hc_elems * cb,
+                               (int)cb, K::W));
+    } else {
+      SLES_TRY(make_tmap(&a.tm, slot(p, 0), K::EPC, p.nk, N, (long long)p.nkp * cb, M, (long long)N * p.nkp * cb,
+                         pass_slots(p), p.hc_elems * cb, K::W, K::RB));
+    }
     a.err = p.flags;
     a.ws = slot(p, 0);
+    a.out = (split && !inv) ? slab_send2(p) : slot(p, 0);
+    a.split = split ? 1 : 0;
+    a.m = M;
+    a.nx = M;
     a.fs = p.hc_elems;
     a.nkp = p.nkp;
     a.nk = p.nk;
     a.nchunks = ychunks<LES>(p);
-    const long long items = (long long)N * ychunks<LES>(p);
+    const long long items = (long long)M * ychunks<LES>(p);
     if (inv) return launch_persistent(k_ypass<Tp, N, FYI<LES>, LES, 1>, items, K::THREADS, K::SMEM, st, a);
     return launch_persistent(k_ypass<Tp, N, FYF, LES, 0>, items, KF::THREADS, KF::SMEM, st, a);
   }
@@ -463,7 +515,7 @@ struct EngineImpl final : Engine {
     a.ws = slot(p, 0);
     a.fs = p.hc_elems;
     a.nkp = p.nkp;
-    a.nlines = (DIM == 3) ? (long long)N * N : N;
+    a.nlines = (DIM == 3) ? (long long)p.slab_m * N : N;
     a.scale = (Tp)(1.0 / (DIM == 3 ? (double)N * N * N : (double)N * N));
     const double dx = 2.0 * 3.141592653589793 / N;  // initialize_domain.py:42
     if (MODEL == M_SMAG) a.cdx2 = (Tp)((p.d.cs * dx) * (p.d.cs * dx));
@@ -541,12 +593,13 @@ struct EngineImpl final : Engine {
     return pipeline(p, les, (const C*)uh, false, (const Tp*)uphys, (const Tp*)cphys, 0, a, st);
   }
 
-  int stage(PlanInfo& p, int s, double dt, const void* ucur, const void* u0, void* u1, void* uout, void* aux,
-            const void* uphys, const void* cphys, int flags, cudaStream_t st, sles_dtctl* ctl = nullptr,
-            int parity = 0) override {
+  // The x-pass arguments of one integrator stage (kind, coefficients, state
+  // pointers).  les / primed may be cleared (the reference's ETD2 drops LES).
+  int stage_args(const PlanInfo& p, int s, double dt, const void* ucur, const void* u0, void* u1, void* uout,
+                 void* aux, int flags, XArgs<Tp>& a, int& les, bool& primed) {
     const auto& d = p.d;
-    int les = d.les_model != SLES_LES_NONE;
-    XArgs<Tp> a = xbase(p);
+    les = d.les_model != SLES_LES_NONE;
+    a = xbase(p);
     a.ucur = (const C*)ucur;
     a.u0 = (const C*)u0;
     a.u1 = (C*)u1;
@@ -554,7 +607,7 @@ struct EngineImpl final : Engine {
     a.aux = (C*)aux;
     a.stage = s;
     a.prep = (flags & STAGE_NO_PREPARE) ? 0 : 1;
-    bool primed = (flags & STAGE_PRIMED) != 0;
+    primed = (flags & STAGE_PRIMED) != 0;
     const int scheme = (flags & STAGE_RK4) ? SLES_RK4 : d.scheme;
     static const double rk4a[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};  // initialize_domain.py:166
     static const double rk4b[3] = {0.5, 0.5, 1.0};                              // initialize_domain.py:167
@@ -592,6 +645,17 @@ struct EngineImpl final : Engine {
     // stage coefficients: the dt multiples, in float64 then rounded (device dt: the same products in-kernel)
     a.c1 = (Tp)(a.m1 * dt);
     a.c2 = (Tp)(a.m2 * dt);
+    return SLES_OK;
+  }
+
+  int stage(PlanInfo& p, int s, double dt, const void* ucur, const void* u0, void* u1, void* uout, void* aux,
+            const void* uphys, const void* cphys, int flags, cudaStream_t st, sles_dtctl* ctl = nullptr,
+            int parity = 0) override {
+    const auto& d = p.d;
+    XArgs<Tp> a;
+    int les = 0;
+    bool primed = false;
+    SLES_TRY(stage_args(p, s, dt, ucur, u0, u1, uout, aux, flags, a, les, primed));
     if (ctl) a.dt_dev = &ctl->dt_step;
     if (flags & STAGE_RECORD_F1) {
       if (!aux) return SLES_ERR_INVALID_ARG;
@@ -604,6 +668,43 @@ struct EngineImpl final : Engine {
     }
     return pipeline(p, les, (const C*)ucur, primed, (const Tp*)uphys, (const Tp*)cphys, 0, a, st,
                     (ctl && s == 0) ? ctl : nullptr, parity);
+  }
+
+  // ---------------- slab decomposition (3D) ----------------
+  int slab_counts(const PlanInfo& p, int* n1, int* n2) const override {
+    const bool les = p.d.les_model != SLES_LES_NONE;
+    *n1 = les ? 6 : 5;  // x-inverse outputs (A_c, B_c; no LES: A_c and the two kx curl parts)
+    *n2 = les ? 6 : 3;  // y-forward outputs (G_c, H_c; no LES: N_c)
+    return DIM == 3 ? SLES_OK : SLES_ERR_UNSUPPORTED;
+  }
+  // inverse x-transforms of the state on this rank's ky rows -> slots [0, n1)
+  int slab_prime(PlanInfo& p, const void* u, cudaStream_t st) override {
+    XArgs<Tp> a0 = xbase(p);
+    a0.fwd = 0;
+    a0.prep = 1;
+    a0.uinv = (const C*)u;
+    return xpass_rt(p, a0, p.d.les_model != SLES_LES_NONE, p.d.parity, st);
+  }
+  // after exchange 1: y inverse (from the exchange buffer), z, y forward (into
+  // the outgoing buffer) on this rank's x planes
+  int slab_middle(PlanInfo& p, unsigned long long* umax, cudaStream_t st) override {
+    const int les = p.d.les_model != SLES_LES_NONE;
+    SLES_TRY(les ? ypass<1>(p, 1, st, true) : ypass<0>(p, 1, st, true));
+    SLES_TRY(zpass_rt(p, les, p.d.les_model, p.d.parity, nullptr, nullptr, 0, st, umax));
+    return les ? ypass<1>(p, 0, st, true) : ypass<0>(p, 0, st, true);
+  }
+  // after exchange 2: the x forward, combine, projection and stage update on
+  // this rank's ky rows, then (unless NO_PREPARE) the x-inverse priming
+  int slab_stage(PlanInfo& p, int s, double dt, const void* ucur, const void* u0, void* u1, void* uout, void* aux,
+                 int flags, cudaStream_t st) override {
+    if (flags & (STAGE_RECORD_F1 | STAGE_PRIMED)) return SLES_ERR_UNSUPPORTED;
+    XArgs<Tp> a;
+    int les = 0;
+    bool primed = false;
+    SLES_TRY(stage_args(p, s, dt, ucur, u0, u1, uout, aux, flags, a, les, primed));
+    if (les != (p.d.les_model != SLES_LES_NONE)) return SLES_ERR_UNSUPPORTED;  // the reference's ETD2 with LES
+    a.fwd = 1;
+    return xpass_rt(p, a, les, p.d.parity, st);
   }
 
   int profile_rhs(PlanInfo& p, const void* uh, void* du, int iters, double* ms, cudaStream_t st) override {
@@ -712,6 +813,9 @@ struct EngineImpl final : Engine {
                        pa.ws_fields, pa.hc_elems * cb, K::W, K::RB));
     a.err = pa.flags;
     a.ws = slot(pa, 0);
+    a.out = slot(pa, 0);
+    a.nx = N;
+    a.m = N;
     a.fs = pa.hc_elems;
     a.nkp = pa.nkp;
     a.nk = pa.nk;

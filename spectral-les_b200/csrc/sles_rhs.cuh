@@ -52,6 +52,7 @@ struct XArgs {
   C* ws;                 // workspace slot 0
   long long fs;          // elements per half-complex field
   int nkp, nk, nchunks;
+  int nsl, ky0;          // 3D: ky slices held (N, or N/P on a slab) and the global index of the first
   int fwd;               // 1: forward part (RHS from the slots), 0: inverse only from uinv
   int prep;              // 1: inverse part (prime the slots for the next evaluation)
   const C* uinv;         // inverse-only source
@@ -323,9 +324,9 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
   F::fill_table_lin(twt);
   __syncthreads();
   F fft;
-  const int nsl = (DIM == 3) ? N : 1;
+  const int nsl = (DIM == 3) ? A.nsl : 1;
   const long long items = (long long)nsl * A.nchunks;
-  const long long ps = (DIM == 3) ? (long long)N * A.nkp : (long long)A.nkp;
+  const long long ps = (DIM == 3) ? (long long)nsl * A.nkp : (long long)A.nkp;  // x stride
   const long long fs = A.fs;
   C* sm = sm0 + l;
   C* ws = A.ws;
@@ -481,14 +482,14 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
 #pragma unroll
       for (int c = 0; c < D; ++c) s[c] = rst[rpos(c, m)];
       kv[0] = kx_at(m);
-      if (DIM == 3) { kv[1] = kc2c(sl, N); kv[D - 1] = col; }
+      if (DIM == 3) { kv[1] = kc2c(A.ky0 + sl, N); kv[D - 1] = col; }
       else kv[1] = col;
       project<Tp, D>(A, s, kv);
 #pragma unroll
       for (int c = 0; c < D; ++c) rst[rpos(c, m)] = s[c];
     }
     // per component: state update, then the inverse transforms of the new state
-    const int kyv = (DIM == 3) ? kc2c(sl, N) : 0;
+    const int kyv = (DIM == 3) ? kc2c(A.ky0 + sl, N) : 0;
 #pragma unroll 1
     for (int c = 0; c < D; ++c) {
       C v[V];
@@ -544,11 +545,16 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
 template <typename Tp>
 struct YArgs {
   using C = typename CT<Tp>::C;
-  CUtensorMap tm;        // workspace slots as y-pass tiles
+  CUtensorMap tm;        // workspace slots as y-pass tiles (split loads: the 5D exchange-buffer map)
   unsigned* err;
   C* ws;
+  C* out;                // where the pass stores (the workspace, or the slab exchange buffer)
   long long fs;
   int nkp, nk, nchunks;
+  int nx;                // x planes held (N, or N/P on a slab)
+  int split;             // slab exchange: 0 none; inverse pass: lines arrive split in P blocks of m rows
+                         // (5D map); forward pass: outputs stored as [slot][P][nx][m][nkp] blocks
+  int m;                 // rows per block (N/P)
 };
 
 // INV = 1: inverse (y1), 0: forward (y2).  ADJ = 1: the adjoint's passes
@@ -573,13 +579,16 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
   F fft;
   F::fill_table(twt);
   __syncthreads();
-  const long long items = (long long)N * A.nchunks;
+  const long long items = (long long)A.nx * A.nchunks;
   const long long mine = (blockIdx.x < items) ? (items - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
   const long long ntiles = mine * NT;
   auto issue = [&](long long t) {
     const long long it = blockIdx.x + (t / NT) * (long long)gridDim.x;
     const int chunk = (int)(it % A.nchunks), x = (int)(it / A.nchunks);
-    ring.issue(t, &A.tm, chunk * W * K::EPC, x, seq_slot<KIND>((int)(t % NT)), K::NBOX, K::RB, K::BOX_BYTES);
+    if (INV && A.split)
+      ring.issue_split(t, &A.tm, chunk * W * K::EPC, x, seq_slot<KIND>((int)(t % NT)), K::NBOX * K::BOX_BYTES);
+    else
+      ring.issue(t, &A.tm, chunk * W * K::EPC, x, seq_slot<KIND>((int)(t % NT)), K::NBOX, K::RB, K::BOX_BYTES);
   };
   if (tid == 0) {
     tma_prefetch_desc(&A.tm);
@@ -607,9 +616,17 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
     const bool ok = col < A.nk;
     const long long base = (long long)x * N * A.nkp + col;
     auto st = [&](int slot, const C (&v)[V]) {
-      if (ok) {
+      if (!ok) return;
+      if (!INV && A.split) {  // row y = b*m + r goes to block b: [slot][b][x][r][kz]
+        const long long bs = (long long)A.nx * A.m * A.nkp;
 #pragma unroll
-        for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
+        for (int m = 0; m < V; ++m) {
+          const int y = j + T * m, b = y / A.m, r = y - b * A.m;
+          A.out[slot * fs + b * bs + ((long long)x * A.m + r) * A.nkp + col] = v[m];
+        }
+      } else {
+#pragma unroll
+        for (int m = 0; m < V; ++m) A.out[slot * fs + base + (j + T * m) * ps] = v[m];
       }
     };
     if (ADJ && !INV) {
@@ -933,6 +950,14 @@ k_zpass(const ZArgs<Tp> A) {
   const int j = tid % T, ln = (tid / T) % LPI, grp = tid / (T * LPI);
   F fft;
   fft.init(j);
+  // line-level exchanges (WS): the real<->half-complex steps take their mirror
+  // bins from the line's lanes by shuffles and their twiddles W_N^k from registers
+  C twr[WS ? V : 1];
+  if constexpr (WS) {
+#pragma unroll
+    for (int m = 0; m < V; ++m) twr[m] = twiddle<Tp>(j + T * m, N, -1);
+  }
+  const unsigned wmask = ((tid | 31) < K::THREADS) ? 0xffffffffu : ((1u << (K::THREADS & 31)) - 1u);
   const long long fs = A.fs;
   Tp* myreg = reg + (grp * LPI + ln) * K::RS;
   C* sm = reinterpret_cast<C*>(myreg);
@@ -981,13 +1006,15 @@ k_zpass(const ZArgs<Tp> A) {
     {
       const C* sb = stage + buf * K::STAGE + ln * NKP;
       C v[V];
-      c2r_pre<F>(v, j, twN, [&](int k) {
+      auto bin = [&](int k) {
         C r = cmk<C>(0, 0);
         if (!ok) return r;
         if (s1 >= 0) r = sb[s1 * LPI * NKP + k];
         if (s2 >= 0) r = cadd(r, cmuli_s(sb[s2 * LPI * NKP + k], sgn * (Tp)k));
         return r;
-      });
+      };
+      if constexpr (WS) c2r_pre_lanes<F>(v, j, twr, bin, wmask);  // mirror bins by shuffles
+      else c2r_pre<F>(v, j, twN, bin);
       fft.template run<+1, WS>(v, j, sm, 1);
       F::template lsync<WS>();  // the region doubles as exchange scratch: all reads done
       C* dst = reinterpret_cast<C*>(myreg);
@@ -1036,9 +1063,11 @@ k_zpass(const ZArgs<Tp> A) {
       fft.template run<-1, WS>(v, j, sm, 1);
       C* out = A.ws + (grp < K::NOUT ? grp : 0) * fs + lo;
       const bool wr = ok && grp < K::NOUT;
-      r2c_post<F, WS>(v, j, sm, 1, twN, [&](int k, C x) {
+      auto put = [&](int k, C x) {
         if (wr) out[k] = x;
-      });
+      };
+      if constexpr (WS) r2c_post_lanes<F>(v, j, twr, put, wmask);
+      else r2c_post<F, WS>(v, j, sm, 1, twN, put);
     }
   }
   if (A.umax) {  // block maximum through the (now idle) line regions, one atomic per block

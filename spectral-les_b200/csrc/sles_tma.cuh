@@ -31,6 +31,15 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+      "%6}], [%7];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_addr(bar))
+      : "memory");
+}
+
 __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
@@ -73,6 +82,16 @@ struct TileRing {
     mbar_arrive_expect_tx(b, box_bytes * nbox);
     for (int k = 0; k < nbox; ++k)
       tma_load_4d(dst + (long long)k * (TE / nbox), map, c0, row, k * rows_per_box, slot, b);
+  }
+  // thread 0: one 5D box {cols, M rows, 1 slice, P blocks, 1 slot} holding a
+  // whole line split in P blocks of M rows (the slab exchange buffer, where
+  // the rows of a line arrive from P ranks); lands as [P][M][W] = [rows][W]
+  __device__ __forceinline__ void issue_split(long long t, const CUtensorMap* map, int c0, int slice, int slot,
+                                              unsigned bytes) {
+    uint64_t* b = &bar[t % NBUF];
+    fence_proxy_async();
+    mbar_arrive_expect_tx(b, bytes);
+    tma_load_5d(tile(t), map, c0, 0, slice, 0, slot, b);
   }
   __device__ __forceinline__ void wait(long long t, unsigned* err) {
     mbar_wait_bounded(&bar[t % NBUF], (unsigned)((t / NBUF) & 1), err);

@@ -18,8 +18,9 @@
 // Stores (new state, primed slots) are plain 8/16-byte global stores, each
 // warp writing whole 64-byte row segments.
 //
-// Tensor maps (4D, 8-byte elements): {nk*EPC columns, N ky rows, N x slices,
-// slots}; box {W*EPC, 1, RB, 1}, so a box lands as [RB x][W] in shared memory.
+// Tensor maps (4D, 8-byte elements): {nk*EPC columns, nsl ky rows, N x slices,
+// slots}; box {W*EPC, 1, RB, 1}, so a box lands as [RB x][W] in shared memory
+// (nsl = N, or N/P ky rows on a slab of a P-rank decomposition).
 // The innermost coordinate is chunk*W*EPC elements = a multiple of 64 bytes.
 #pragma once
 #include "sles_rhs.cuh"
@@ -79,7 +80,7 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
   __syncthreads();
   const int l = tid % W, j = tid / W;
   F fft;
-  const long long items = (long long)N * A.nchunks;
+  const long long items = (long long)A.nsl * A.nchunks;
   const long long mine = (blockIdx.x < items) ? (items - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
   constexpr int NTF = LES ? 6 : D;
   const int nst = A.need_uc + A.need_u0 + A.need_u1;
@@ -133,7 +134,7 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
     for (int m = 0; m < V; ++m) v[m] = p[T * m * W];
     release(1);
   };
-  const long long ps = (long long)N * A.nkp, fs = A.fs;
+  const long long ps = (long long)A.nsl * A.nkp, fs = A.fs;  // x stride
   C* sm = sm0 + l;
   C* ws = A.ws;
   const StageCoef<Tp> SC = stage_coef<Tp>(A);
@@ -194,7 +195,7 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
       }
     }
     // mask + projection, in registers
-    const int kyv = kc2c(sl, N);
+    const int kyv = kc2c(A.ky0 + sl, N);
 #pragma unroll
     for (int m = 0; m < V; ++m) {
       C s[D];

@@ -29,6 +29,8 @@ EXPORTED = [
     "sles_plan_variant_count", "sles_plan_get_variant", "sles_plan_set_variant", "sles_stage_ctl",
     "sles_plan_check", "sles_selftest_wait_timeout", "sles_selftest_wait_timeout_word", "sles_adjoint_check",
     "sles_static_workspace_check", "sles_static_workspace_selftest_timeout",
+    "sles_plan_set_slab", "sles_slab_info", "sles_slab_buffers", "sles_slab_prime", "sles_slab_middle",
+    "sles_slab_stage",
 ]
 DT_DONE, DT_SNAPSHOT, DT_NAN, DT_TOO_SMALL = 1, 2, 4, 8
 
@@ -48,6 +50,13 @@ class PlanDesc(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("n", ctypes.c_int), ("dtype", ctypes.c_int),
                 ("les_model", ctypes.c_int), ("scheme", ctypes.c_int), ("parity", ctypes.c_int),
                 ("nu", ctypes.c_double), ("cs", ctypes.c_double), ("forcing", ctypes.c_double)]
+
+
+class SlabLayout(ctypes.Structure):
+    """sles_slab_layout (include/sles.h)."""
+    _fields_ = [("nranks", ctypes.c_int32), ("rank", ctypes.c_int32), ("m", ctypes.c_int32),
+                ("n_exchange1", ctypes.c_int32), ("n_exchange2", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("block_elems", ctypes.c_int64), ("field_elems", ctypes.c_int64)]
 
 
 class Layout(ctypes.Structure):
@@ -103,6 +112,13 @@ def load_library(path: str = LIB_PATH):
         "sles_plan_variant_count": (i, [vp, i]),
         "sles_plan_get_variant": (i, [vp, i]),
         "sles_plan_set_variant": (i, [vp, i, i]),
+        "sles_plan_set_slab": (i, [vp, i, i]),
+        "sles_slab_info": (i, [vp, ctypes.POINTER(SlabLayout)]),
+        "sles_slab_buffers": (i, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                  ctypes.POINTER(vp)]),
+        "sles_slab_prime": (i, [vp, vp, vp]),
+        "sles_slab_middle": (i, [vp, vp, vp]),
+        "sles_slab_stage": (i, [vp, i, d, vp, vp, vp, vp, vp, i, vp]),
         "sles_adjoint_workspace_bytes": (ctypes.c_size_t, [vp]),
         "sles_adjoint_seed": (i, [vp, vp, d, vp, vp, vp, vp]),
         "sles_adjoint_prime": (i, [vp, vp, vp, vp, vp]),
@@ -133,7 +149,7 @@ def stream_handle(device=None):
 class Plan:
     """Owns a ``sles_plan`` and its workspace (from torch's caching allocator)."""
 
-    def __init__(self, dim, n, dtype, les_model, scheme, parity, nu, cs, forcing, device):
+    def __init__(self, dim, n, dtype, les_model, scheme, parity, nu, cs, forcing, device, slab=None):
         if not torch.cuda.is_available():
             raise RuntimeError("the spectral-LES B200 path needs a CUDA device; there is no CPU fallback")
         L = load_library()
@@ -144,6 +160,8 @@ class Plan:
         h = ctypes.c_void_p()
         check(L.sles_plan_create(ctypes.byref(self.desc), ctypes.byref(h)), "sles_plan_create")
         self.h = h
+        if slab is not None:  # (nranks, rank): this rank's slab of a decomposed domain
+            check(L.sles_plan_set_slab(h, int(slab[0]), int(slab[1])), "sles_plan_set_slab")
         lay = Layout()
         check(L.sles_plan_layout(h, ctypes.byref(lay)), "sles_plan_layout")
         self.hc_elems, self.real_elems, self.nkp, self.nk = lay.hc_elems, lay.real_elems, lay.nkp, lay.nk
@@ -156,6 +174,28 @@ class Plan:
         self._ws_ptr = self.workspace.data_ptr() + off
         check(L.sles_plan_set_workspace(h, ctypes.c_void_p(self._ws_ptr), ctypes.c_size_t(nbytes)),
               "sles_plan_set_workspace")
+
+    # slab decomposition (include/sles.h): layout, exchange buffers, the three pass groups
+    def slab_info(self):
+        lay = SlabLayout()
+        check(self.L.sles_slab_info(self.h, ctypes.byref(lay)), "sles_slab_info")
+        return lay
+
+    def slab_buffers(self):
+        """Device addresses (send1, recv1, send2, recv2) inside the workspace."""
+        p = [ctypes.c_void_p() for _ in range(4)]
+        check(self.L.sles_slab_buffers(self.h, *[ctypes.byref(x) for x in p]), "sles_slab_buffers")
+        return [int(x.value) for x in p]
+
+    def slab_prime(self, u):
+        check(self.L.sles_slab_prime(self.h, ptr(u), stream_handle(self.device)), "sles_slab_prime")
+
+    def slab_middle(self, umax_bits=None):
+        check(self.L.sles_slab_middle(self.h, ptr(umax_bits), stream_handle(self.device)), "sles_slab_middle")
+
+    def slab_stage(self, stage, dt, ucur, u0, u1, uout, aux=None, flags=0):
+        check(self.L.sles_slab_stage(self.h, int(stage), float(dt), ptr(ucur), ptr(u0), ptr(u1), ptr(uout), ptr(aux),
+                                     int(flags), stream_handle(self.device)), "sles_slab_stage")
 
     def variant_count(self, pass_=PASS_X):
         return int(self.L.sles_plan_variant_count(self.h, int(pass_)))
