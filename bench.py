@@ -658,6 +658,34 @@ def bench_ensemble(rank, steps=200):
     return out
 
 
+def bench_kernels(case, n, precision, rank, xvar=-1):
+    """Mean ms per launch of each kernel class of one RHS evaluation
+    (sles_profile_rhs, CUDA events, 20 evaluations) and its algorithmic GB/s."""
+    from sles import ETD2_method
+    d = bench_case_domain(case, n, precision, rank)
+    if xvar >= 0:
+        d._plan.set_variant(xvar)
+    kms = d._plan.profile_rhs(d._s_uhat, d._new_hc(3), 20)
+    names = ["x_inverse", "y_inverse", "z_fused", "y_forward", "x_forward_combine"]
+    les = case != "none"
+    nf = (9, 15, 18, 15, 18) if les else (5, 8, 9, 6, 8)
+    fbytes = float(n) * n * (n // 2 + 1) * (8 if precision == "float32" else 16)
+    return {"case": case, "n": n, "precision": precision, "x_variant": d._plan.get_variant(0),
+            "kernel_ms": {k: round(t, 4) for k, t in zip(names, kms)},
+            "kernel_gbs": {k: round(b * fbytes / (t * 1e-3) / 1e9, 1) for k, b, t in zip(names, nf, kms)}}
+
+
+def bench_case_domain(case, n, precision, rank):
+    if case == "vreman_etd2":
+        return make_domain(n, precision, rank, method="ETD2", les="vreman", nu=5e-5, cs=math.sqrt(0.07 / 2.5),
+                           dt=5e-4, k0=6.0, parity=False)
+    if case == "smag_rk4":
+        d = make_domain(n, precision, rank, method="RK4")
+        d.U_hat1[...] = d.U_hat
+        return d
+    return make_domain(n, precision, rank)
+
+
 def bench_steps(case, n, precision, steps, warmup, rank, xvar=-1):
     """A plain stepping run of one workload (for ncu launch lists and
     captures): the Smagorinsky recipe with the reference RK3 or RK4, or the
@@ -725,7 +753,7 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (use the default or cached kernel variants)")
-    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble", "driver", "fft", "steps"],
+    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble", "driver", "fft", "steps", "kernels"],
                     help="run one extra block alone and print it (profiling; not a bench line); 'steps': "
                          "--case at --n stepped --steps times after --warmup (for ncu launch lists)")
     ap.add_argument("--case", default="smag_rk3", choices=["smag_rk3", "vreman_etd2", "smag_rk4"],
@@ -768,6 +796,7 @@ def main():
         fn = {"n512": lambda: bench_512(peak, rank), "adjoint": lambda: bench_adjoint(rank),
               "ensemble": lambda: bench_ensemble(rank), "driver": lambda: bench_driver(rank),
               "fft": lambda: bench_fft(rank),
+              "kernels": lambda: bench_kernels(args.case, args.n, args.precision, rank, args.xvar),
               "steps": lambda: bench_steps(args.case, args.n, args.precision, args.steps, args.warmup, rank,
                                            args.xvar)}[args.only]
         print(json.dumps({"only": args.only, "result": fn()}))

@@ -503,6 +503,12 @@ struct EngineImpl final : Engine {
     a.nk = p.nk;
     a.nchunks = ychunks<LES>(p);
     const long long items = (long long)M * ychunks<LES>(p);
+    if constexpr (DIM == 3) {
+      if (split) {
+        if (inv) return launch_persistent(k_ypass<Tp, N, FYI<LES>, LES, 1, 0, 1>, items, K::THREADS, K::SMEM, st, a);
+        return launch_persistent(k_ypass<Tp, N, FYF, LES, 0, 0, 1>, items, KF::THREADS, KF::SMEM, st, a);
+      }
+    }
     if (inv) return launch_persistent(k_ypass<Tp, N, FYI<LES>, LES, 1>, items, K::THREADS, K::SMEM, st, a);
     return launch_persistent(k_ypass<Tp, N, FYF, LES, 0>, items, KF::THREADS, KF::SMEM, st, a);
   }

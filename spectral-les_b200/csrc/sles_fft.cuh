@@ -418,78 +418,4 @@ __device__ __forceinline__ void r2c_post(typename F::C (&v)[F::V], int j, typena
   }
 }
 
-// ---------------------------------------------------------------------------
-// The same pre/post steps with the mirror bins exchanged between the line's
-// lanes by warp shuffles (the T lanes of a line consecutive inside one warp).
-// With k = j + T m held by lane j at register m, the bin (L - k) mod L sits
-// in lane (T - j) mod T at register V-1-m (j != 0) and in lane 0 itself at
-// register (V - m) mod V (j = 0).  `wmask`: the warp's lanes present in the
-// block (all of them call these functions together).  tw[m] = W_N^{j + T m}.
-// ---------------------------------------------------------------------------
-template <class F>
-__device__ __forceinline__ typename F::C lane_mirror(const typename F::C (&a)[F::V], int j, int m, unsigned wmask) {
-  using C = typename F::C;
-  constexpr int T = F::T, V = F::V;
-  const C own = a[(V - m) % V];
-  if constexpr (T == 1) {
-    return own;
-  } else {
-    const C x = a[V - 1 - m];
-    const int lane = (int)(threadIdx.x & 31u);
-    const int src = lane - j + (T - j) % T;
-    C r;
-    r.x = __shfl_sync(wmask, x.x, src);
-    r.y = __shfl_sync(wmask, x.y, src);
-    return j == 0 ? own : r;
-  }
-}
-
-// c2r pre-step: X(k) returns the half-complex input bin k (called for this
-// lane's bins and, on lane 0, for k = L); imaginary parts of bins 0 and L
-// are discarded as in c2r_pre.
-template <class F, class Src>
-__device__ __forceinline__ void c2r_pre_lanes(typename F::C (&v)[F::V], int j, const typename F::C (&tw)[F::V],
-                                              Src X, unsigned wmask) {
-  using C = typename F::C;
-  constexpr int T = F::T, V = F::V;
-  C a[V];
-#pragma unroll
-  for (int m = 0; m < V; ++m) a[m] = X(j + T * m);
-  C nyq = cmk<C>(0, 0);
-  if (j == 0) nyq = X(F::L);
-#pragma unroll
-  for (int m = 0; m < V; ++m) {
-    C b = lane_mirror<F>(a, j, m, wmask);
-    C x = a[m];
-    if (m == 0 && j == 0) {
-      b = nyq;
-      x.y = 0;
-      b.y = 0;
-    }
-    C e = cadd(x, cconj(b));
-    C o = cmulc(csub(x, cconj(b)), tw[m]);
-    v[m] = cadd(e, cmuli(o));
-  }
-}
-
-// r2c post-step: v holds Z = FFT_L(z); emits out(k, X_k) for this lane's k
-// and, on lane 0, out(L, X_L).
-template <class F, class Dst>
-__device__ __forceinline__ void r2c_post_lanes(const typename F::C (&v)[F::V], int j, const typename F::C (&tw)[F::V],
-                                               Dst out, unsigned wmask) {
-  using C = typename F::C;
-  using Tp = decltype(C::x);
-  constexpr int T = F::T, V = F::V;
-#pragma unroll
-  for (int m = 0; m < V; ++m) {
-    const int k = j + T * m;
-    const C z = v[m];
-    const C zc = cconj(lane_mirror<F>(v, j, m, wmask));
-    C s = cadd(z, zc), d = csub(z, zc);
-    C t = cmulmi(cmul(tw[m], d));
-    out(k, cmk<C>((Tp)0.5 * (s.x + t.x), (Tp)0.5 * (s.y + t.y)));
-    if (k == 0) out(F::L, cmk<C>(z.x - z.y, (Tp)0));
-  }
-}
-
 }  // namespace sles

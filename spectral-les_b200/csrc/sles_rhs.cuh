@@ -561,7 +561,9 @@ struct YArgs {
 // (discrete adjoint of the RHS, see sles_adjoint.cuh): the inverse carries two
 // groups (the recomputed state and the cotangent), the forward contracts
 // Z_j - i ky A2_j.
-template <typename Tp, int N, class F, int LES, int INV, int ADJ = 0>
+// SPLIT = 1: the slab exchange layouts (A.split; see YArgs), compiled apart so
+// the whole-grid kernels carry none of its addressing
+template <typename Tp, int N, class F, int LES, int INV, int ADJ = 0, int SPLIT = 0>
 __global__ void __launch_bounds__(TGeo<Tp, N, F, true, 0, LES>::THREADS, TGeo<Tp, N, F, true, 0, LES>::MINB)
 k_ypass(const __grid_constant__ YArgs<Tp> A) {
   using K = TGeo<Tp, N, F, true, 0, LES>;
@@ -585,7 +587,7 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
   auto issue = [&](long long t) {
     const long long it = blockIdx.x + (t / NT) * (long long)gridDim.x;
     const int chunk = (int)(it % A.nchunks), x = (int)(it / A.nchunks);
-    if (INV && A.split)
+    if (INV && SPLIT)
       ring.issue_split(t, &A.tm, chunk * W * K::EPC, x, seq_slot<KIND>((int)(t % NT)), K::NBOX * K::BOX_BYTES);
     else
       ring.issue(t, &A.tm, chunk * W * K::EPC, x, seq_slot<KIND>((int)(t % NT)), K::NBOX, K::RB, K::BOX_BYTES);
@@ -617,7 +619,7 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
     const long long base = (long long)x * N * A.nkp + col;
     auto st = [&](int slot, const C (&v)[V]) {
       if (!ok) return;
-      if (!INV && A.split) {  // row y = b*m + r goes to block b: [slot][b][x][r][kz]
+      if (!INV && SPLIT) {  // row y = b*m + r goes to block b: [slot][b][x][r][kz]
         const long long bs = (long long)A.nx * A.m * A.nkp;
 #pragma unroll
         for (int m = 0; m < V; ++m) {
@@ -626,7 +628,7 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
         }
       } else {
 #pragma unroll
-        for (int m = 0; m < V; ++m) A.out[slot * fs + base + (j + T * m) * ps] = v[m];
+        for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
       }
     };
     if (ADJ && !INV) {
@@ -950,14 +952,6 @@ k_zpass(const ZArgs<Tp> A) {
   const int j = tid % T, ln = (tid / T) % LPI, grp = tid / (T * LPI);
   F fft;
   fft.init(j);
-  // line-level exchanges (WS): the real<->half-complex steps take their mirror
-  // bins from the line's lanes by shuffles and their twiddles W_N^k from registers
-  C twr[WS ? V : 1];
-  if constexpr (WS) {
-#pragma unroll
-    for (int m = 0; m < V; ++m) twr[m] = twiddle<Tp>(j + T * m, N, -1);
-  }
-  const unsigned wmask = ((tid | 31) < K::THREADS) ? 0xffffffffu : ((1u << (K::THREADS & 31)) - 1u);
   const long long fs = A.fs;
   Tp* myreg = reg + (grp * LPI + ln) * K::RS;
   C* sm = reinterpret_cast<C*>(myreg);
@@ -1006,15 +1000,13 @@ k_zpass(const ZArgs<Tp> A) {
     {
       const C* sb = stage + buf * K::STAGE + ln * NKP;
       C v[V];
-      auto bin = [&](int k) {
+      c2r_pre<F>(v, j, twN, [&](int k) {
         C r = cmk<C>(0, 0);
         if (!ok) return r;
         if (s1 >= 0) r = sb[s1 * LPI * NKP + k];
         if (s2 >= 0) r = cadd(r, cmuli_s(sb[s2 * LPI * NKP + k], sgn * (Tp)k));
         return r;
-      };
-      if constexpr (WS) c2r_pre_lanes<F>(v, j, twr, bin, wmask);  // mirror bins by shuffles
-      else c2r_pre<F>(v, j, twN, bin);
+      });
       fft.template run<+1, WS>(v, j, sm, 1);
       F::template lsync<WS>();  // the region doubles as exchange scratch: all reads done
       C* dst = reinterpret_cast<C*>(myreg);
@@ -1063,11 +1055,9 @@ k_zpass(const ZArgs<Tp> A) {
       fft.template run<-1, WS>(v, j, sm, 1);
       C* out = A.ws + (grp < K::NOUT ? grp : 0) * fs + lo;
       const bool wr = ok && grp < K::NOUT;
-      auto put = [&](int k, C x) {
+      r2c_post<F, WS>(v, j, sm, 1, twN, [&](int k, C x) {
         if (wr) out[k] = x;
-      };
-      if constexpr (WS) r2c_post_lanes<F>(v, j, twr, put, wmask);
-      else r2c_post<F, WS>(v, j, sm, 1, twN, put);
+      });
     }
   }
   if (A.umax) {  // block maximum through the (now idle) line regions, one atomic per block
