@@ -424,7 +424,7 @@ struct EngineImpl final : Engine {
     if constexpr (!HAS_XTMA) {
       return xpass_v<LES, PAR2D, 0>(p, a, st);
     } else {
-      using F = typename WithPad<typename PlanLo<Tp, N>::F, SLES_X_PADD>::F;
+      using F = FXV<2>;  // 32-byte tile rows: the exchange padded every 8 points, as variant 2
       using K = XTGeo<Tp, N, F>;
       XTArgs<Tp> P{};
       a.nchunks = (p.nk + K::W - 1) / K::W;

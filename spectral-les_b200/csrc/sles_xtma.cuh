@@ -10,9 +10,10 @@
 //    [x rows][W columns] at fixed ky, prefetched NBUF tiles ahead into a ring
 //    of shared buffers completed on mbarriers (one elected thread issues,
 //    bounded waits), as the y passes stream theirs;
-//  * the three projected components stay in registers (each thread owns the
-//    same cyclic positions of every component, so the projection needs no
-//    shared stash);
+//  * the three projected components wait in a shared stash [3][N][W] between
+//    the forward transforms and the per-component update (kept in registers
+//    they spill: the update and inverse transforms of one component run while
+//    the other two wait);
 //  * the state tiles of a component are read straight from the ring inside
 //    the update loop, then released together.
 // Stores (new state, primed slots) are plain 8/16-byte global stores, each
@@ -39,7 +40,7 @@ struct XTArgs {
 template <typename Tp, int N, class F>
 struct XTGeo {
   using C = typename CT<Tp>::C;
-  static constexpr int W = (sizeof(Tp) == 4) ? 8 : 4;  // 64-byte tile rows
+  static constexpr int W = (sizeof(Tp) == 4) ? 4 : 2;  // 32-byte tile rows
   static constexpr int EPC = sizeof(C) / 8;
   static constexpr int T = F::T, V = F::V;
   static constexpr int THREADS = W * T;
@@ -48,19 +49,21 @@ struct XTGeo {
   static constexpr int TE = N * W;
   static constexpr unsigned BOX_BYTES = RB * W * sizeof(C);
   static constexpr int SCR = F::XLEN * W;
-  static constexpr long long FIXED = 1024 + ((long long)SCR + F::LIN_LEN) * (long long)sizeof(C);
+  static constexpr int STASH = 3 * TE;  // projected components [3][N][W]
+  static constexpr long long FIXED = 1024 + ((long long)STASH + SCR + F::LIN_LEN) * (long long)sizeof(C);
   // tile buffers that fit next to the scratch when `minb` blocks share an SM
   // (228 KB of shared memory per SM, 1 KB reserved per block)
   static constexpr long long nbuf_for(int minb) {
     return ((228LL / minb - 1) * 1024 - FIXED) / ((long long)TE * (long long)sizeof(C));
   }
-  // blocks per SM: the most (4, 2, 1) that keep at least 4 ring buffers
+  // blocks per SM: the most (4, 3, 2, 1) that keep at least 4 ring buffers
   static constexpr int MINB = (THREADS * 4 <= 1024 && nbuf_for(4) >= 4) ? 4
-                              : ((THREADS * 2 <= 1024 && nbuf_for(2) >= 4) ? 2 : 1);
+                              : ((THREADS * 3 <= 1024 && nbuf_for(3) >= 4) ? 3
+                                 : ((THREADS * 2 <= 1024 && nbuf_for(2) >= 4) ? 2 : 1));
   static constexpr int NBUF = nbuf_for(MINB) > 6 ? 6 : (int)nbuf_for(MINB);
   static_assert(NBUF >= 4, "the ring must hold a component's state tiles plus lookahead");
   using Ring = TileRing<C, NBUF, TE>;
-  static constexpr size_t SMEM = Ring::bytes() + ((size_t)SCR + F::LIN_LEN) * sizeof(C);
+  static constexpr size_t SMEM = Ring::bytes() + ((size_t)STASH + SCR + F::LIN_LEN) * sizeof(C);
 };
 
 template <typename Tp, int N, class F, int LES, int ETD>
@@ -74,7 +77,8 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
   typename K::Ring ring;
   const int tid = threadIdx.x;
   ring.init(smem_raw, tid);
-  C* sm0 = reinterpret_cast<C*>(smem_raw + K::Ring::bytes());  // exchange scratch
+  C* rst = reinterpret_cast<C*>(smem_raw + K::Ring::bytes());  // projected components [3][N][W]
+  C* sm0 = rst + K::STASH;                                       // exchange scratch
   C* twt = sm0 + K::SCR;                                         // linear twiddle table
   F::fill_table_lin(twt);
   __syncthreads();
@@ -181,37 +185,41 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
       continue;
     }
     // forward x-transforms; the x part of div(tau) joins in spectral space
-    C r3[D][V];
-#pragma unroll
+    // (component loops not unrolled: each transform's code exists once)
+    auto rpos = [&](int c, int m) { return c * K::TE + (j + T * m) * W + l; };
+#pragma unroll 1
     for (int c = 0; c < D; ++c) {
-      take(r3[c]);
-      fft.template run_tab<-1, true>(r3[c], j, sm, W, twt);
+      C v[V];
+      take(v);
+      fft.template run_tab<-1, true>(v, j, sm, W, twt);
       if (LES) {  // + 2i kx F_cx
         C h[V];
         take(h);
         fft.template run_tab<-1, true>(h, j, sm, W, twt);
 #pragma unroll
-        for (int m = 0; m < V; ++m) r3[c][m] = cadd(r3[c][m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
+        for (int m = 0; m < V; ++m) v[m] = cadd(v[m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
       }
+#pragma unroll
+      for (int m = 0; m < V; ++m) rst[rpos(c, m)] = v[m];
     }
-    // mask + projection, in registers
+    // mask + projection (each thread revisits only its own stash positions)
     const int kyv = kc2c(A.ky0 + sl, N);
 #pragma unroll
     for (int m = 0; m < V; ++m) {
-      C s[D];
+      C s3[D];
       int kv[D];
 #pragma unroll
-      for (int c = 0; c < D; ++c) s[c] = r3[c][m];
+      for (int c = 0; c < D; ++c) s3[c] = rst[rpos(c, m)];
       kv[0] = kx_at(m);
       kv[1] = kyv;
       kv[2] = col;
-      project<Tp, D>(A, s, kv);
+      project<Tp, D>(A, s3, kv);
 #pragma unroll
-      for (int c = 0; c < D; ++c) r3[c][m] = s[c];
+      for (int c = 0; c < D; ++c) rst[rpos(c, m)] = s3[c];
     }
     // per component: the stage update from the state tiles in the ring, then
     // the inverse transforms of the new state
-#pragma unroll
+#pragma unroll 1
     for (int c = 0; c < D; ++c) {
       const C* pu = nullptr;
       const C* p0 = nullptr;
@@ -232,7 +240,7 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
           const C ucm = pu ? pu[T * m * W] : cmk<C>(0, 0);
           const C u0m = p0 ? p0[T * m * W] : ucm;
           const C u1m = p1 ? p1[T * m * W] : cmk<C>(0, 0);
-          v[m] = update_component<Tp, ETD>(A, SC, c, r3[c][m], ucm, u0m, u1m, k2, off);
+          v[m] = update_component<Tp, ETD>(A, SC, c, rst[rpos(c, m)], ucm, u0m, u1m, k2, off);
         }
       } else {
 #pragma unroll
