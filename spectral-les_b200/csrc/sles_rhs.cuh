@@ -830,7 +830,14 @@ struct ZGeo {
   static constexpr int RS = 2 * LS;
   static_assert(RS >= N, "region must hold a physical line");
   static_assert((size_t)NG * LPI * RS * sizeof(Tp) >= (size_t)THREADS * sizeof(double), "regions hold the u_max partials");
-  static constexpr int STAGE = NIN * LPI * NKP;   // complex elements per staging buffer
+  // staging: NIN slot blocks of LPI lines; consecutive blocks start half the
+  // bank space (64 bytes mod 128) apart, so the two line groups of a half warp
+  // reading neighbouring slots hit disjoint banks
+  static constexpr int SLOTS = LPI * NKP;
+  static constexpr int SLOT_STRIDE =
+      SLOTS + (int)(((64 - (long long)SLOTS * (long long)sizeof(C)) % 128 + 128) % 128 / (long long)sizeof(C));
+  static_assert((SLOT_STRIDE * sizeof(C)) % 16 == 0, "bulk copies need 16-byte aligned slot blocks");
+  static constexpr int STAGE = NIN * SLOT_STRIDE;  // complex elements per staging buffer
   static constexpr size_t OFF_TW = 16;
   static constexpr size_t OFF_STAGE = OFF_TW + (size_t)L * sizeof(C);
   static constexpr size_t OFF_REG = OFF_STAGE + 2 * (size_t)STAGE * sizeof(C);
@@ -983,7 +990,7 @@ k_zpass(const ZArgs<Tp> A) {
     fence_proxy_async();
     mbar_arrive_expect_tx(&bar[buf], bytes * K::NIN);
     for (int s = 0; s < K::NIN; ++s)
-      bulk_g2s(stage + buf * K::STAGE + s * LPI * NKP, A.ws + s * fs + l0 * A.nkp, bytes, &bar[buf]);
+      bulk_g2s(stage + buf * K::STAGE + s * K::SLOT_STRIDE, A.ws + s * fs + l0 * A.nkp, bytes, &bar[buf]);
   };
   if (tid == 0 && blockIdx.x < nbi) issue(blockIdx.x, 0);
   double lmax = -INFINITY;  // max of u over this thread's points (when A.umax)
@@ -1003,8 +1010,8 @@ k_zpass(const ZArgs<Tp> A) {
       c2r_pre<F>(v, j, twN, [&](int k) {
         C r = cmk<C>(0, 0);
         if (!ok) return r;
-        if (s1 >= 0) r = sb[s1 * LPI * NKP + k];
-        if (s2 >= 0) r = cadd(r, cmuli_s(sb[s2 * LPI * NKP + k], sgn * (Tp)k));
+        if (s1 >= 0) r = sb[s1 * K::SLOT_STRIDE + k];
+        if (s2 >= 0) r = cadd(r, cmuli_s(sb[s2 * K::SLOT_STRIDE + k], sgn * (Tp)k));
         return r;
       });
       fft.template run<+1, WS>(v, j, sm, 1);
@@ -1047,7 +1054,7 @@ k_zpass(const ZArgs<Tp> A) {
     __syncthreads();
     // ---- phase C: r2c of product `grp` (with block-wide line barriers, groups
     // >= NOUT run idle for them; with line-level barriers they skip)
-    if (WS || grp < K::NOUT) {
+    if (!WS || grp < K::NOUT) {
       C v[V];
       const C* src = reinterpret_cast<const C*>(myreg);
 #pragma unroll
