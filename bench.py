@@ -177,9 +177,11 @@ def tune_domain(d):
     from sles import autotune
     if not os.environ.get("SLES_TUNE_CACHE"):
         os.environ["SLES_TUNE_CACHE"] = os.path.join(tempfile.gettempdir(), "sles_bench_tune_%d.json" % os.getpid())
-    times = autotune.tune(d) if TUNE else {}
-    return {"x_pass_variant": d._plan.get_variant(0), "ms_per_step_by_variant": {str(k): round(v, 4)
-                                                                                  for k, v in times.items()}}
+    report = autotune.tune(d) if TUNE else {}
+    names = {0: "x", 1: "y", 2: "z"}
+    return {"variants": {names[p]: d._plan.get_variant(p) for p in names},
+            "ms_per_step_by_variant": {names[p]: {str(k): round(v, 4) for k, v in t.items()}
+                                       for p, t in report.items()}}
 
 
 def rel_l2(a, b):

@@ -86,10 +86,13 @@ int sles_plan_layout(const sles_plan* plan, sles_layout* out);
  * which times each.  Every variant computes the same arithmetic (results agree
  * to the last bit or, where the compiler contracts a*b+c differently, to round-off).
  *   SLES_PASS_X: the x pass (stage update); variants 0..count-1
- * sles_plan_variant_count returns 0 for a pass without variants;
+ *   SLES_PASS_Y: the y passes (tile width 8 or 16 columns; variant 1 only for
+ *                the float32 3D grids 128, 256, 512, where the count is 2)
+ *   SLES_PASS_Z: the fused z pass (1 or 2 z lines per work item; idem)
+ * sles_plan_variant_count returns 0 for an invalid pass (1: no alternative);
  * sles_plan_get_variant returns -1 for an invalid pass.
  */
-enum { SLES_PASS_X = 0 };
+enum { SLES_PASS_X = 0, SLES_PASS_Y = 1, SLES_PASS_Z = 2 };
 int sles_plan_variant_count(const sles_plan* plan, int pass);
 int sles_plan_get_variant(const sles_plan* plan, int pass);
 int sles_plan_set_variant(sles_plan* plan, int pass, int variant);

@@ -81,6 +81,7 @@ int sles_plan_create(const sles_plan_desc* d, sles_plan** out) {
   I.flags = nullptr;
   I.scal = nullptr;
   I.xvar = eng->default_xvar();
+  I.yvar = I.zvar = 0;
   I.slab_p = 1;
   I.slab_r = 0;
   I.slab_m = d->n;
@@ -125,18 +126,28 @@ int sles_slab_info(const sles_plan* p, sles_slab_layout* out) {
 
 int sles_plan_variant_count(const sles_plan* p, int pass) {
   if (!p) return 0;
-  return pass == SLES_PASS_X ? sles::X_VARIANTS : 0;
+  return p->eng->variant_count(pass);
 }
 
 int sles_plan_get_variant(const sles_plan* p, int pass) {
-  if (!p || pass != SLES_PASS_X) return -1;
-  return p->info.xvar;
+  if (!p) return -1;
+  switch (pass) {
+    case SLES_PASS_X: return p->info.xvar;
+    case SLES_PASS_Y: return p->info.yvar;
+    case SLES_PASS_Z: return p->info.zvar;
+    default: return -1;
+  }
 }
 
 int sles_plan_set_variant(sles_plan* p, int pass, int variant) {
-  if (!p || pass != SLES_PASS_X) return SLES_ERR_INVALID_ARG;
-  if (variant < 0 || variant >= sles::X_VARIANTS) return SLES_ERR_INVALID_ARG;
-  p->info.xvar = variant;
+  if (!p) return SLES_ERR_INVALID_ARG;
+  if (variant < 0 || variant >= p->eng->variant_count(pass)) return SLES_ERR_INVALID_ARG;
+  switch (pass) {
+    case SLES_PASS_X: p->info.xvar = variant; break;
+    case SLES_PASS_Y: p->info.yvar = variant; break;
+    case SLES_PASS_Z: p->info.zvar = variant; break;
+    default: return SLES_ERR_INVALID_ARG;
+  }
   return SLES_OK;
 }
 

@@ -29,6 +29,7 @@ struct PlanInfo {
   unsigned* flags;       // device error word inside the workspace
   double* scal;          // device scalar scratch inside the workspace (64 doubles)
   int xvar;              // x-pass variant (XGeo), set by default or by the autotuner
+  int yvar, zvar;        // y- and z-pass variants (tile width, lines per work item)
   // slab decomposition over P ranks (3D): this rank holds ky rows [r*m, (r+1)*m)
   // of spectral fields and x planes [r*m, (r+1)*m) of physical ones (m = N/P);
   // P = 1, m = N: the whole grid
@@ -49,6 +50,7 @@ struct Engine {
   virtual ~Engine() {}
   virtual int ws_fields_needed(const PlanInfo& p) const = 0;
   virtual int default_xvar() const = 0;
+  virtual int variant_count(int pass) const = 0;  // SLES_PASS_X / _Y / _Z
   virtual int fft_r2c(PlanInfo& p, const void* in, void* out, int nf, cudaStream_t st) = 0;
   virtual int fft_c2r(PlanInfo& p, const void* in, void* out, int nf, cudaStream_t st) = 0;
   virtual int velocity_curl(PlanInfo& p, const void* uh, void* u, void* curl, cudaStream_t st) = 0;
@@ -331,6 +333,12 @@ struct EngineImpl final : Engine {
   // x-pass variant used until a caller (the autotuner) sets another: the
   // fastest in a timing sweep of every size on a B200 (RK3 Smagorinsky and
   // RK4 without LES; see sles/autotune.py)
+  int variant_count(int pass) const override {
+    if (pass == 0) return X_VARIANTS;
+    if (pass == 1) return HAS_YVAR ? 2 : 1;
+    if (pass == 2) return HAS_ZVAR ? 2 : 1;
+    return 0;
+  }
   int default_xvar() const override {
     if (sizeof(Tp) == 8) return (DIM == 2 && N >= 1024) ? 0 : (DIM == 2 ? 2 : 1);
     if (DIM == 2) return 2;
@@ -476,13 +484,30 @@ struct EngineImpl final : Engine {
   static C* slab_recv1(const PlanInfo& p) { return slot(p, pass_slots(p)); }
   static C* slab_send2(const PlanInfo& p) { return slot(p, pass_slots(p) + p.slab_n1); }
 
+  // y-pass variant 1 (float32 3D grids 128, 256, 512): the other tile width
+  // (8 <-> 16 columns); elsewhere one variant
+  static constexpr bool HAS_YVAR = sizeof(Tp) == 4 && DIM == 3 && (N == 128 || N == 256 || N == 512);
+  template <int LES>
+  static constexpr int yw_alt() { return YGeoI<LES>::W == 8 ? 16 : 8; }
+
   // split: on a slab (P > 1 or an explicit exchange), the inverse pass reads the
   // exchange buffer and the forward pass stores into the outgoing one
   template <int LES>
   int ypass(const PlanInfo& p, int inv, cudaStream_t st, bool split = false) {
-    if (DIM != 3) return SLES_OK;
-    using K = YGeoI<LES>;  // tile geometry (the tensor map) is the same for the forward plan
-    using KF = YGeoF<LES>;
+    if constexpr (DIM != 3) {
+      return SLES_OK;
+    } else {
+      if constexpr (HAS_YVAR) {
+        if (p.yvar == 1 && !split) return ypass_w<LES, yw_alt<LES>()>(p, inv, st, false);
+      }
+      return ypass_w<LES, 0>(p, inv, st, split);
+    }
+  }
+  template <int LES, int YW>
+  int ypass_w(const PlanInfo& p, int inv, cudaStream_t st, bool split) {
+    using K = TGeo<Tp, N, FYI<LES>, true, 0, LES, YW>;  // tile geometry (the tensor map) shared by both plans
+    using KF = TGeo<Tp, N, FYF, true, 0, LES, YW>;
+    static_assert(K::W == KF::W, "one tile width for both y directions");
     YArgs<Tp> a{};
     const long long cb = sizeof(C);
     const int M = p.slab_m;
@@ -502,22 +527,31 @@ struct EngineImpl final : Engine {
     a.fs = p.hc_elems;
     a.nkp = p.nkp;
     a.nk = p.nk;
-    a.nchunks = ychunks<LES>(p);
-    const long long items = (long long)M * ychunks<LES>(p);
-    if constexpr (DIM == 3) {
-      if (split) {
-        if (inv) return launch_persistent(k_ypass<Tp, N, FYI<LES>, LES, 1, 0, 1>, items, K::THREADS, K::SMEM, st, a);
-        return launch_persistent(k_ypass<Tp, N, FYF, LES, 0, 0, 1>, items, KF::THREADS, KF::SMEM, st, a);
-      }
+    a.nchunks = (p.nk + K::W - 1) / K::W;
+    const long long items = (long long)M * a.nchunks;
+    if (split) {
+      if (inv) return launch_persistent(k_ypass<Tp, N, FYI<LES>, LES, 1, 0, 1, YW>, items, K::THREADS, K::SMEM, st, a);
+      return launch_persistent(k_ypass<Tp, N, FYF, LES, 0, 0, 1, YW>, items, KF::THREADS, KF::SMEM, st, a);
     }
-    if (inv) return launch_persistent(k_ypass<Tp, N, FYI<LES>, LES, 1>, items, K::THREADS, K::SMEM, st, a);
-    return launch_persistent(k_ypass<Tp, N, FYF, LES, 0>, items, KF::THREADS, KF::SMEM, st, a);
+    if (inv) return launch_persistent(k_ypass<Tp, N, FYI<LES>, LES, 1, 0, 0, YW>, items, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_ypass<Tp, N, FYF, LES, 0, 0, 0, YW>, items, KF::THREADS, KF::SMEM, st, a);
   }
 
+  // z-pass variant 1 (float32 3D grids 128, 256, 512): twice the z lines per work item
+  static constexpr bool HAS_ZVAR = sizeof(Tp) == 4 && DIM == 3 && (N == 128 || N == 256 || N == 512);
   template <int LES, int MODEL, int PAR2D>
   int zpass(const PlanInfo& p, const Tp* uphys, const Tp* cphys, int stress_only, cudaStream_t st,
             unsigned long long* umax) {
-    using K = ZGeo<Tp, N, DIM, LES, PAR2D, LPI>;
+    if constexpr (HAS_ZVAR) {
+      if (p.zvar == 1) return zpass_l<LES, MODEL, PAR2D, 2 * LPI>(p, uphys, cphys, stress_only, st, umax);
+    }
+    return zpass_l<LES, MODEL, PAR2D, LPI>(p, uphys, cphys, stress_only, st, umax);
+  }
+
+  template <int LES, int MODEL, int PAR2D, int ZL>
+  int zpass_l(const PlanInfo& p, const Tp* uphys, const Tp* cphys, int stress_only, cudaStream_t st,
+              unsigned long long* umax) {
+    using K = ZGeo<Tp, N, DIM, LES, PAR2D, ZL>;
     ZArgs<Tp> a{};
     a.ws = slot(p, 0);
     a.fs = p.hc_elems;
@@ -534,7 +568,8 @@ struct EngineImpl final : Engine {
     a.err = p.flags;
     a.umax = umax;
     if (p.nkp != K::NKP) return SLES_ERR_INVALID_ARG;
-    return launch_persistent(k_zpass<Tp, N, DIM, LES, MODEL, PAR2D, LPI>, (a.nlines + LPI - 1) / LPI, K::THREADS, K::SMEM, st, a);
+    return launch_persistent(k_zpass<Tp, N, DIM, LES, MODEL, PAR2D, ZL>, (a.nlines + ZL - 1) / ZL, K::THREADS, K::SMEM,
+                             st, a);
   }
   int zpass_rt(const PlanInfo& p, int les, int model, int par2d, const Tp* uphys, const Tp* cphys, int so,
                cudaStream_t st, unsigned long long* umax = nullptr) {

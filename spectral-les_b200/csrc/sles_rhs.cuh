@@ -197,7 +197,8 @@ __device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& 
 // Strided-axis pass geometry: one work item (W lines of N points) per block
 // iteration; tiles arrive by TMA into a ring of NBUF buffers.
 // ---------------------------------------------------------------------------
-template <typename Tp, int N, class F, bool RING = true, int NBUF_SET = 0, int WIDE = 0>
+// WSET > 0 sets the tile width (the y-pass variant with the other width)
+template <typename Tp, int N, class F, bool RING = true, int NBUF_SET = 0, int WIDE = 0, int WSET = 0>
 struct TGeo {
   using C = typename CT<Tp>::C;
 #ifndef SLES_Y_W
@@ -211,7 +212,7 @@ struct TGeo {
   // 1.75 + 2.01 ms against 2.21 + 2.06; the passes without LES and all passes
   // at 256^3 were slower with the wider rows); FP64: 64-byte rows
   static constexpr int W =
-      (sizeof(Tp) == 4) ? (SLES_Y_W > 0 ? SLES_Y_W : ((N == 512 && WIDE) ? 16 : 8)) : 4;
+      WSET > 0 ? WSET : ((sizeof(Tp) == 4) ? (SLES_Y_W > 0 ? SLES_Y_W : ((N == 512 && WIDE) ? 16 : 8)) : 4);
   static constexpr int EPC = sizeof(C) / 8;                 // 8-byte tensor elements per complex
   static constexpr int T = F::T, V = F::V;
   static constexpr int THREADS = W * T;
@@ -563,10 +564,10 @@ struct YArgs {
 // Z_j - i ky A2_j.
 // SPLIT = 1: the slab exchange layouts (A.split; see YArgs), compiled apart so
 // the whole-grid kernels carry none of its addressing
-template <typename Tp, int N, class F, int LES, int INV, int ADJ = 0, int SPLIT = 0>
-__global__ void __launch_bounds__(TGeo<Tp, N, F, true, 0, LES>::THREADS, TGeo<Tp, N, F, true, 0, LES>::MINB)
+template <typename Tp, int N, class F, int LES, int INV, int ADJ = 0, int SPLIT = 0, int YW = 0>
+__global__ void __launch_bounds__(TGeo<Tp, N, F, true, 0, LES, YW>::THREADS, TGeo<Tp, N, F, true, 0, LES, YW>::MINB)
 k_ypass(const __grid_constant__ YArgs<Tp> A) {
-  using K = TGeo<Tp, N, F, true, 0, LES>;
+  using K = TGeo<Tp, N, F, true, 0, LES, YW>;
   using C = typename CT<Tp>::C;
   constexpr int T = K::T, V = K::V, W = K::W;
   constexpr int KIND = ADJ ? (INV ? 6 : 7) : (INV ? (LES ? 0 : 1) : (LES ? 2 : 3));

@@ -43,7 +43,8 @@ class DtCtl(ctypes.Structure):
                 ("umax_bits", ctypes.c_uint64 * 2), ("flags", ctypes.c_uint32), ("paused", ctypes.c_uint32),
                 ("nsteps", ctypes.c_uint32), ("t_init", ctypes.c_uint32), ("resumed", ctypes.c_uint32),
                 ("reserved", ctypes.c_uint32)]
-PASS_X = 0
+PASS_X, PASS_Y, PASS_Z = 0, 1, 2
+PASSES = (PASS_X, PASS_Y, PASS_Z)
 
 
 class PlanDesc(ctypes.Structure):

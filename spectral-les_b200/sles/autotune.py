@@ -1,17 +1,22 @@
 """Autotuner for the fused passes' kernel variants.
 
-Some passes are compiled in several tile geometries (``sles_plan_variant_count``
-in include/sles.h); all variants compute the same arithmetic (identical results
-up to the compiler's floating-point contraction) and differ only in speed,
-which depends on the grid size, precision, closure and scheme.
+The passes are compiled in several tile geometries (``sles_plan_variant_count``
+in include/sles.h): the x pass in four (tile width, tile ring or direct
+loads, shared stash), the y passes in two tile widths (8 or 16 columns) and
+the z pass with one or two z lines per work item (the last two on the float32
+3D grids 128, 256 and 512).  All variants compute the same arithmetic
+(identical results up to the compiler's floating-point contraction) and differ
+only in speed, which depends on the grid size, precision, closure and scheme.
 ``tune(domain)`` times whole steps of the domain's own scheme with each
-variant on scratch copies of the state (the domain's state is not advanced),
-keeps the fastest, and records the choice in a JSON cache keyed by device,
-dimension, grid, precision, closure and scheme.  New domains with a cached key
-pick the recorded variant up at construction (``apply_cached``).
+variant of each pass on scratch copies of the state (the domain's state is
+not advanced), one pass at a time with the others at their current best
+(x, then y, then z), keeps the fastest, and records the choices in a JSON
+cache keyed by device, dimension, grid, precision, closure and scheme.  New
+domains with a cached key pick the recorded variants up at construction
+(``apply_cached``).
 
     from sles import autotune
-    times = autotune.tune(domain)      # {variant: ms per step}; domain now uses the fastest
+    times = autotune.tune(domain)      # {pass: {variant: ms per step}}; domain now uses the fastest
 
 The cache file is ``$SLES_TUNE_CACHE`` if set, else
 ``~/.cache/sles_b200/autotune.json``.
@@ -101,19 +106,19 @@ def _step_fn(domain):
     return step
 
 
-def tune(domain, steps=4, repeats=3, save=True):
-    """Time ``steps`` steps per x-pass variant (best of ``repeats``), set the
-    fastest on the domain's plan and record it.  Returns {variant: ms/step}."""
+def tune(domain, steps=4, repeats=3, save=True, passes=nat.PASSES):
+    """Time ``steps`` steps per variant (best of ``repeats``) of each pass with
+    more than one variant, set the fastest on the domain's plan and record the
+    choices.  Returns {pass: {variant: ms/step}} for the passes tuned."""
     plan = domain._plan
-    nv = plan.variant_count(nat.PASS_X)
-    if nv <= 1:
+    todo = [p for p in passes if plan.variant_count(p) > 1]
+    if not todo:
         return {}
     step = _step_fn(domain)
     st = torch.cuda.current_stream(plan.device)
-    times = {}
-    for v in range(nv):
-        plan.set_variant(v, nat.PASS_X)
-        step(False)  # first launch of this variant (attributes, occupancy query)
+
+    def time_it():
+        step(False)  # first launch of this combination (attributes, occupancy query)
         best = None
         for _ in range(repeats):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -124,13 +129,22 @@ def tune(domain, steps=4, repeats=3, save=True):
             e1.synchronize()
             ms = e0.elapsed_time(e1) / steps
             best = ms if best is None else min(best, ms)
-        times[v] = best
-    win = min(times, key=times.get)
-    plan.set_variant(win, nat.PASS_X)
+        return best
+
+    report = {}
+    for p in todo:
+        times = {}
+        for v in range(plan.variant_count(p)):
+            plan.set_variant(v, p)
+            times[v] = time_it()
+        win = min(times, key=times.get)
+        plan.set_variant(win, p)
+        report[p] = times
     domain._primed = None  # the workspace holds the scratch run's transforms
     if save:
         table = _load()
-        table[plan_key(plan, domain.method)] = {"variants": {str(nat.PASS_X): win},
-                                                 "ms_per_step": {str(k): round(t, 4) for k, t in times.items()}}
+        table[plan_key(plan, domain.method)] = {
+            "variants": {str(p): plan.get_variant(p) for p in passes if plan.variant_count(p) >= 1},
+            "ms_per_step": {str(p): {str(k): round(t, 4) for k, t in tt.items()} for p, tt in report.items()}}
         _save(table)
-    return times
+    return report

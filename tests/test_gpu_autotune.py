@@ -76,7 +76,8 @@ def test_tune_records_and_reapplies(tmp_path, monkeypatch):
     monkeypatch.setenv("SLES_TUNE_CACHE", str(tmp_path / "tune.json"))
     d = _dom(3, 64, "float32", "Smagorinsky", "RK3", True)
     before = d.U_hat.clone()
-    times = autotune.tune(d, steps=2, repeats=2)
+    report = autotune.tune(d, steps=2, repeats=2)
+    times = report[nat.PASS_X]
     assert set(times) == set(range(NV)) and all(t > 0 for t in times.values())
     win = min(times, key=times.get)
     assert d._plan.get_variant(nat.PASS_X) == win
@@ -92,3 +93,31 @@ def test_tune_records_and_reapplies(tmp_path, monkeypatch):
         RK3_method.solveForNextTimestep(d)
         RK3_method.solveForNextTimestep(d3)
     assert torch.equal(d.U_hat, d3.U_hat)
+
+
+@pytest.mark.parametrize("n,les,method", [(128, "Smagorinsky", "RK3"), (256, "Smagorinsky", "RK3"),
+                                          (128, None, "RK4")])
+def test_y_and_z_variants_agree_and_are_tuned(n, les, method, tmp_path, monkeypatch):
+    """The y-pass tile widths and the z-pass lines per item give the same
+    states (float32 bit-identical: the same arithmetic per line), and tune()
+    records a choice for every pass with variants."""
+    ref = None
+    for py, pz in ((0, 0), (1, 0), (0, 1), (1, 1)):
+        d = _dom(3, n, "float32", les, method, True)
+        assert d._plan.variant_count(nat.PASS_Y) == 2 and d._plan.variant_count(nat.PASS_Z) == 2
+        d._plan.set_variant(py, nat.PASS_Y)
+        d._plan.set_variant(pz, nat.PASS_Z)
+        for _ in range(2):
+            STEP[method](d)
+        d._plan.check()
+        u = d.U_hat.clone()
+        if ref is None:
+            ref = u
+        else:
+            assert torch.equal(u, ref), "y/z variants (%d, %d) differ" % (py, pz)
+    monkeypatch.setenv("SLES_TUNE_CACHE", str(tmp_path / "tune.json"))
+    report = autotune.tune(d, steps=1, repeats=1)
+    assert set(report) == {nat.PASS_X, nat.PASS_Y, nat.PASS_Z}
+    table = json.loads((tmp_path / "tune.json").read_text())
+    ent = table[autotune.plan_key(d._plan, method)]["variants"]
+    assert {int(k) for k in ent} == {nat.PASS_X, nat.PASS_Y, nat.PASS_Z}
