@@ -137,6 +137,22 @@ typedef struct sles_slab_layout {
   int64_t field_elems;            /* complex elements per field on this rank: N*m*nkp */
 } sles_slab_layout;
 int sles_plan_set_slab(sles_plan* plan, int nranks, int rank);
+/*
+ * Ensemble batch (no counterpart in the reference; the reference runs one
+ * domain per process): the plan steps `nmembers` independent domains of its
+ * grid, scheme, closure and precision together, every pass one launch over
+ * the work items of all members.  Each field argument of sles_stage / sles_rhs
+ * then holds the members one after another inside each component:
+ * [component][member][layout of one domain] (sles_plan_layout's hc_elems
+ * counts all members).  nu_dev / cs_dev: device arrays of nmembers float64
+ * values (each member's viscosity and C_s; NULL: the descriptor's value for
+ * all), read by the kernels, so they must stay valid while the plan runs.
+ * Call before sles_plan_set_workspace (the workspace scales with nmembers);
+ * not with sles_plan_set_slab.  On a batched plan only sles_stage (without
+ * u_phys / curl_phys) and sles_rhs run; the other entry points return
+ * SLES_ERR_STATE.
+ */
+int sles_plan_set_batch(sles_plan* plan, int nmembers, const double* nu_dev, const double* cs_dev);
 int sles_slab_info(const sles_plan* plan, sles_slab_layout* out);
 int sles_slab_buffers(sles_plan* plan, void** send1, void** recv1, void** send2, void** recv2);
 int sles_slab_prime(sles_plan* plan, const void* u_state, void* stream);

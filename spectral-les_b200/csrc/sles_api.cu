@@ -86,14 +86,29 @@ int sles_plan_create(const sles_plan_desc* d, sles_plan** out) {
   I.slab_r = 0;
   I.slab_m = d->n;
   I.slab_n1 = I.slab_n2 = 0;
+  I.nmem = 1;
+  I.mnu = I.mcs = nullptr;
   *out = p;
+  return SLES_OK;
+}
+
+int sles_plan_set_batch(sles_plan* p, int nmembers, const double* nu_dev, const double* cs_dev) {
+  if (!p) return SLES_ERR_INVALID_ARG;
+  sles::PlanInfo& I = p->info;
+  if (I.ws || I.slab_n1 || I.nmem != 1) return SLES_ERR_STATE;  // before the workspace; not on a slab; once
+  if (nmembers < 1 || nmembers > 4096) return SLES_ERR_INVALID_ARG;
+  I.nmem = nmembers;
+  I.mnu = nu_dev;
+  I.mcs = cs_dev;
+  I.hc_elems *= nmembers;
+  I.real_elems *= nmembers;
   return SLES_OK;
 }
 
 int sles_plan_set_slab(sles_plan* p, int nranks, int rank) {
   if (!p) return SLES_ERR_INVALID_ARG;
   sles::PlanInfo& I = p->info;
-  if (I.ws) return SLES_ERR_STATE;  // the layout must be fixed before the workspace is attached
+  if (I.ws || I.nmem != 1) return SLES_ERR_STATE;  // before the workspace; not on a member batch
   if (I.d.dim != 3) return SLES_ERR_UNSUPPORTED;
   if (nranks < 1 || rank < 0 || rank >= nranks || I.d.n % nranks != 0) return SLES_ERR_INVALID_ARG;
   const int m = I.d.n / nranks;
@@ -198,10 +213,17 @@ static int ready(sles_plan* p) {
   return SLES_OK;
 }
 
-// entry points that work on the whole grid: not on a plan set to a slab
+// entry points that work on the whole grid: not on a plan set to a slab, nor
+// (except the stage and RHS calls) on a batch of ensemble members
 static int ready_full(sles_plan* p) {
   if (int s = ready(p)) return s;
+  if (p->info.slab_n1 != 0 || p->info.nmem != 1) return SLES_ERR_STATE;
+  return SLES_OK;
+}
+static int ready_batch(sles_plan* p, const void* uphys, const void* cphys) {
+  if (int s = ready(p)) return s;
   if (p->info.slab_n1 != 0) return SLES_ERR_STATE;
+  if (p->info.nmem != 1 && (uphys || cphys)) return SLES_ERR_UNSUPPORTED;  // stored fields are per domain
   return SLES_OK;
 }
 
@@ -230,7 +252,7 @@ int sles_velocity_gradient(sles_plan* p, const void* uh, void* grad, void* strea
 }
 
 int sles_rhs(sles_plan* p, const void* uh, const void* uphys, const void* cphys, void* du, void* f1, void* stream) {
-  if (int s = ready_full(p)) return s;
+  if (int s = ready_batch(p, uphys, cphys)) return s;
   if (!uh || !du) return SLES_ERR_INVALID_ARG;
   if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
   return p->eng->rhs(p->info, uh, uphys, cphys, du, f1, (cudaStream_t)stream);
@@ -238,7 +260,7 @@ int sles_rhs(sles_plan* p, const void* uh, const void* uphys, const void* cphys,
 
 int sles_stage(sles_plan* p, int stage, double dt, const void* ucur, const void* u0, void* u1, void* uout, void* aux,
                const void* uphys, const void* cphys, int flags, void* stream) {
-  if (int s = ready_full(p)) return s;
+  if (int s = ready_batch(p, uphys, cphys)) return s;
   if (!ucur || !uout || !(dt == dt)) return SLES_ERR_INVALID_ARG;
   if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
   const int scheme = (flags & sles::STAGE_RK4) ? SLES_RK4 : p->info.d.scheme;
@@ -354,7 +376,7 @@ size_t sles_adjoint_workspace_bytes(const sles_plan* p) {
 static int adjoint_info(sles_plan* p, void* adj_ws, sles::PlanInfo* out) {
   if (!p || !adj_ws) return SLES_ERR_INVALID_ARG;
   if (p->info.d.dim != 3) return SLES_ERR_UNSUPPORTED;
-  if (p->info.slab_n1 != 0) return SLES_ERR_STATE;
+  if (p->info.slab_n1 != 0 || p->info.nmem != 1) return SLES_ERR_STATE;
   if (((uintptr_t)adj_ws) % 256 != 0) return SLES_ERR_INVALID_ARG;
   *out = p->info;
   out->ws = adj_ws;
@@ -464,7 +486,7 @@ int static_ws_address(void** out) {
 extern "C" int sles_rhs_static_workspace(sles_plan* p, const void* uh, const void* uphys, const void* cphys,
                                          void* du, void* f1, void* stream) {
   if (!p || !uh || !du) return SLES_ERR_INVALID_ARG;
-  if (p->info.slab_n1 != 0) return SLES_ERR_STATE;
+  if (p->info.slab_n1 != 0 || p->info.nmem != 1) return SLES_ERR_STATE;
   if (sles_plan_workspace_bytes(p) > (size_t)SLES_STATIC_WORKSPACE_BYTES) return SLES_ERR_WORKSPACE;
   if (p->info.d.dim == 2 && p->info.d.les_model == SLES_LES_VREMAN && p->info.d.parity) return SLES_ERR_UNSUPPORTED;
   void* ws = nullptr;

@@ -35,6 +35,11 @@ struct PlanInfo {
   // P = 1, m = N: the whole grid
   int slab_p, slab_r, slab_m;
   int slab_n1, slab_n2;  // fields of the two exchanges (x-inverse outputs, y-forward outputs)
+  // ensemble batch: nmem members of this plan's grid stepped together; every
+  // field holds the members one after another (hc_elems counts all of them)
+  int nmem;
+  const double* mnu;     // per-member nu (device), or null
+  const double* mcs;     // per-member C_s (device), or null
 };
 
 // workspace header: error word + scalar scratch, then the diagnostics area,
@@ -402,6 +407,9 @@ struct EngineImpl final : Engine {
     a.nu_d = p.d.nu;
     a.nsl = p.slab_m;
     a.ky0 = p.slab_r * p.slab_m;
+    a.nmem = p.nmem;
+    a.mstride = p.hc_elems / p.nmem;
+    a.mnu = p.mnu;
     return a;
   }
 
@@ -444,14 +452,15 @@ struct EngineImpl final : Engine {
       const long long fsb = p.hc_elems * cb;
       // {columns, ky rows, x slices, slots}; box {W columns, 1 ky row, RB x rows, 1 slot}
       auto mk = [&](CUtensorMap* m, const void* base, long long nslot) {
-        return make_tmap_box(m, base, K::EPC, p.nk, a.nsl, row, N, slice, nslot, fsb, K::W, 1, K::RB);
+        return make_tmap_box(m, base, K::EPC, p.nk, a.nsl, row, (long long)p.nmem * N, slice, nslot, fsb, K::W, 1,
+                             K::RB);
       };
       SLES_TRY(mk(&P.tws, slot(p, 0), p.ws_fields));
       const void* cur = a.fwd ? (const void*)a.ucur : (const void*)a.uinv;
       SLES_TRY(mk(&P.tcur, cur ? cur : slot(p, 0), 3));
       SLES_TRY(mk(&P.t0, a.need_u0 ? (const void*)a.u0 : slot(p, 0), 3));
       SLES_TRY(mk(&P.t1, a.need_u1 ? (const void*)a.u1 : slot(p, 0), 3));
-      const long long items = (long long)a.nsl * a.nchunks;
+      const long long items = (long long)a.nmem * a.nsl * a.nchunks;
       if (a.kind == KX_ETD2P || a.kind == KX_ETD2C) {
         if (LES) return launch_persistent(k_xpass_tma<Tp, N, F, 1, 1>, items, K::THREADS, K::SMEM, st, P);
         return launch_persistent(k_xpass_tma<Tp, N, F, 0, 1>, items, K::THREADS, K::SMEM, st, P);
@@ -466,7 +475,7 @@ struct EngineImpl final : Engine {
     a.nchunks = xchunks<XV>(p);
     set_needs(a);
     a.err = p.flags;
-    const long long items = (long long)(DIM == 3 ? a.nsl : 1) * a.nchunks;
+    const long long items = (long long)a.nmem * (DIM == 3 ? a.nsl : 1) * a.nchunks;
     if (a.kind == KX_ETD2P || a.kind == KX_ETD2C)
       return launch_persistent(k_xpass<Tp, N, FXV<XV>, DIM, LES, PAR2D, 1, XV>, items, K::THREADS, K::SMEM, st, a);
     return launch_persistent(k_xpass<Tp, N, FXV<XV>, DIM, LES, PAR2D, 0, XV>, items, K::THREADS, K::SMEM, st, a);
@@ -510,7 +519,7 @@ struct EngineImpl final : Engine {
     static_assert(K::W == KF::W, "one tile width for both y directions");
     YArgs<Tp> a{};
     const long long cb = sizeof(C);
-    const int M = p.slab_m;
+    const int M = p.slab_m * p.nmem;  // x planes held: a slab's, or every batched member's
     if (split && inv) {
       SLES_TRY(make_tmap_split(&a.tm, slab_recv1(p), K::EPC, p.nk, p.nkp, M, p.slab_p, p.slab_n1, p.hc_elems * cb,
                                (int)cb, K::W));
@@ -556,7 +565,11 @@ struct EngineImpl final : Engine {
     a.ws = slot(p, 0);
     a.fs = p.hc_elems;
     a.nkp = p.nkp;
-    a.nlines = (DIM == 3) ? (long long)p.slab_m * N : N;
+    a.lpm = (DIM == 3) ? (long long)p.slab_m * N : N;
+    a.nlines = a.lpm * p.nmem;
+    a.mcs = p.mcs;
+    a.dx = 2.0 * 3.141592653589793 / N;
+    a.vreman = MODEL == M_VREMAN ? 1 : 0;
     a.scale = (Tp)(1.0 / (DIM == 3 ? (double)N * N * N : (double)N * N));
     const double dx = 2.0 * 3.141592653589793 / N;  // initialize_domain.py:42
     if (MODEL == M_SMAG) a.cdx2 = (Tp)((p.d.cs * dx) * (p.d.cs * dx));

@@ -53,6 +53,9 @@ struct XArgs {
   long long fs;          // elements per half-complex field
   int nkp, nk, nchunks;
   int nsl, ky0;          // 3D: ky slices held (N, or N/P on a slab) and the global index of the first
+  int nmem;              // ensemble members batched in the plan (1: a single domain)
+  long long mstride;     // elements between two members' parts of a field
+  const double* mnu;     // per-member viscosity (device, nmem values) or null: nu_d for all
   int fwd;               // 1: forward part (RHS from the slots), 0: inverse only from uinv
   int prep;              // 1: inverse part (prime the slots for the next evaluation)
   const C* uinv;         // inverse-only source
@@ -115,11 +118,13 @@ __device__ __forceinline__ void project(const XArgs<Tp>& A, typename CT<Tp>::C (
 // or ETD2's previous F1).  Writes uout/u1/aux and returns the new state.
 // ETD = 0 drops the exponential schemes (their float64 weights) from the
 // kernel, which keeps the Runge-Kutta kernels' register count down.
+// nud: the member's viscosity (float64; the working precision rounds it once).
 template <typename Tp, int ETD>
 __device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& A, const StageCoef<Tp>& K, int c,
                                                               typename CT<Tp>::C R,
                                                               typename CT<Tp>::C uc, typename CT<Tp>::C u0,
-                                                              typename CT<Tp>::C u1, int k2, long long off) {
+                                                              typename CT<Tp>::C u1, int k2, long long off,
+                                                              double nud) {
   using C = typename CT<Tp>::C;
   const long long o = c * A.fs + off;
   if (A.kind == KX_RAW) {
@@ -131,11 +136,11 @@ __device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& 
   C un;
   if (ETD && (A.kind == KX_ETD2P || A.kind == KX_ETD2C)) {
     // parity: src/ETD2_method.py:16-29; corrected: Cox & Matthews (2002) eq. 22
-    const double z = K.dt * A.nu_d * (double)k2;
-    const double E = exp(-K.dt * A.nu_d * (double)k2);
+    const double z = K.dt * nud * (double)k2;
+    const double E = exp(-K.dt * nud * (double)k2);
     double w1, w0;
     if (A.kind == KX_ETD2P) {
-      const double nk2 = A.nu_d * (double)k2;
+      const double nk2 = nud * (double)k2;
       const double den = (k2 == 0) ? 1.0 : K.dt * (nk2 * nk2);
       w1 = ((1.0 - z) + 2.0 * z) / den;
       w0 = (-E + 1.0 - z) / den;
@@ -155,7 +160,7 @@ __device__ __forceinline__ typename CT<Tp>::C update_component(const XArgs<Tp>& 
     A.uout[o] = un;
     return un;
   }
-  const C dU = csub(R, cscale(uc, A.nu * (Tp)k2));  // (nu * K2) * U_hat, RK4_method.py:67-68
+  const C dU = csub(R, cscale(uc, (Tp)nud * (Tp)k2));  // (nu * K2) * U_hat, RK4_method.py:67-68
   switch (A.kind) {
     case KX_RK4:  // RK4_method.py:20-27
       if (A.stage < 3) {
@@ -326,7 +331,7 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
   __syncthreads();
   F fft;
   const int nsl = (DIM == 3) ? A.nsl : 1;
-  const long long items = (long long)nsl * A.nchunks;
+  const long long items = (long long)A.nmem * nsl * A.nchunks;
   const long long ps = (DIM == 3) ? (long long)nsl * A.nkp : (long long)A.nkp;  // x stride
   const long long fs = A.fs;
   C* sm = sm0 + l;
@@ -355,7 +360,8 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
       if (it2 < items) {
         const int col2 = (int)(it2 % A.nchunks) * W + l;
         const bool ok2 = col2 < A.nk;
-        const C* src = tile_src((int)(t % TPI)) + (it2 / A.nchunks) * A.nkp + (ok2 ? col2 : 0);
+        const long long r2 = it2 / A.nchunks;  // member * nsl + slice
+        const C* src = tile_src((int)(t % TPI)) + (r2 / nsl) * A.mstride + (r2 % nsl) * A.nkp + (ok2 ? col2 : 0);
         C* dst = ring + (int)(t % NB) * K::TE + j * W + l;
 #pragma unroll
         for (int m = 0; m < V; ++m) cp_async_el<sizeof(C)>(dst + T * m * W, src + (j + T * m) * ps, ok2);
@@ -368,10 +374,14 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
   }
   for (long long it = blockIdx.x; it < items; it += gridDim.x) {  // persistent over work items
     const int chunk = (int)(it % A.nchunks);
-    const int sl = (int)(it / A.nchunks);  // ky slice (3D); 0 in 2D
+    const long long rest = it / A.nchunks;
+    const int sl = (int)(rest % nsl);      // ky slice (3D); 0 in 2D
+    const int mem = (int)(rest / nsl);     // ensemble member
     const int col = chunk * W + l;
     const bool ok = col < A.nk;
-    const long long base = (long long)sl * A.nkp + col;
+    const long long mbase = (long long)mem * A.mstride;
+    const long long base = mbase + (long long)sl * A.nkp + col;
+    const double nud = A.mnu ? A.mnu[mem] : A.nu_d;
     // next tile of the sequence (its source is implied by the sequence position)
     auto take = [&](C (&v)[V], const C* src, int slot) {
       if constexpr (NB > 0) {
@@ -425,7 +435,7 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
     // thread copies exactly the positions it later reads: no block barrier)
     auto sissue = [&](int c) {
       if constexpr (K::SB > 0) {
-        const long long so = c * fs + (long long)sl * A.nkp + (ok ? col : 0);
+        const long long so = c * fs + mbase + (long long)sl * A.nkp + (ok ? col : 0);
         C* d0 = ring + j * W + l;
 #pragma unroll
         for (int m = 0; m < V; ++m) {
@@ -528,7 +538,7 @@ k_xpass(const __grid_constant__ XArgs<Tp> A) {
             u0m = A.need_u0 ? A.u0[c * fs + off] : ucm;
             u1m = A.need_u1 ? A.u1[c * fs + off] : cmk<C>(0, 0);
           }
-          v[m] = update_component<Tp, ETD>(A, SC, c, rst[rpos(c, m)], ucm, u0m, u1m, k2, off);
+          v[m] = update_component<Tp, ETD>(A, SC, c, rst[rpos(c, m)], ucm, u0m, u1m, k2, off, nud);
         }
       } else {
 #pragma unroll
@@ -774,6 +784,10 @@ struct ZArgs {
   int stress_only;       // 1: drop u x omega (evaluates the LES stress alone)
   unsigned* err;         // error word (bounded-wait timeouts)
   unsigned long long* umax;  // non-null: max over components and points of u (ordered encoding)
+  const double* mcs;     // batched members: per-member C_s (device) or null: cdx2 for all
+  long long lpm;         // lines per member
+  double dx;             // grid spacing (with mcs: cdx2 = (Cs dx)^2, Vreman 2.5 Cs^2 dx^2)
+  int vreman;
 };
 
 // order-preserving encoding of a double as an unsigned 64-bit integer (for atomicMax)
@@ -1046,7 +1060,12 @@ k_zpass(const ZArgs<Tp> A) {
 #pragma unroll
         for (int c = 0; c < DIM; ++c) lmax = fmax(lmax, (double)(uo ? uo[c] : reg[c * SFS + sp]));
       }
-      z_pointwise<Tp, DIM, LES, MODEL, PAR2D>(reg, SFS, sp, uo, co, A.cdx2);
+      Tp cdx2 = A.cdx2;
+      if (LES && A.mcs) {  // the member's C_s (the host's float64 products, rounded once)
+        const double cs = A.mcs[pl / A.lpm];
+        cdx2 = A.vreman ? (Tp)(2.5 * cs * cs * A.dx * A.dx) : (Tp)((cs * A.dx) * (cs * A.dx));
+      }
+      z_pointwise<Tp, DIM, LES, MODEL, PAR2D>(reg, SFS, sp, uo, co, cdx2);
       if (A.stress_only) {
 #pragma unroll
         for (int c = 0; c < DIM; ++c) reg[c * SFS + sp] = (Tp)0;

@@ -74,14 +74,15 @@ struct TileRing {
   }
   // thread 0: the same with the box rows along the slice axis (dim 2) at the
   // fixed row `row` (dim 1): x-pass tiles [x][W] at one ky
-  __device__ __forceinline__ void issue_rows(long long t, const CUtensorMap* map, int c0, int row, int slot,
-                                             int nbox, int rows_per_box, unsigned box_bytes) {
+  // (slice0: the first slice of the line, e.g. a batched member's offset)
+  __device__ __forceinline__ void issue_rows(long long t, const CUtensorMap* map, int c0, int row, int slice0,
+                                             int slot, int nbox, int rows_per_box, unsigned box_bytes) {
     uint64_t* b = &bar[t % NBUF];
     C* dst = tile(t);
     fence_proxy_async();
     mbar_arrive_expect_tx(b, box_bytes * nbox);
     for (int k = 0; k < nbox; ++k)
-      tma_load_4d(dst + (long long)k * (TE / nbox), map, c0, row, k * rows_per_box, slot, b);
+      tma_load_4d(dst + (long long)k * (TE / nbox), map, c0, row, slice0 + k * rows_per_box, slot, b);
   }
   // thread 0: one 5D box {cols, M rows, 1 slice, P blocks, 1 slot} holding a
   // whole line split in P blocks of M rows (the slab exchange buffer, where

@@ -84,7 +84,7 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
   __syncthreads();
   const int l = tid % W, j = tid / W;
   F fft;
-  const long long items = (long long)A.nsl * A.nchunks;
+  const long long items = (long long)A.nmem * A.nsl * A.nchunks;
   const long long mine = (blockIdx.x < items) ? (items - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
   constexpr int NTF = LES ? 6 : D;
   const int nst = A.need_uc + A.need_u0 + A.need_u1;
@@ -93,7 +93,9 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
   // tile `k` of an item's sequence: forward slots, then per component the state tiles
   auto issue = [&](long long t) {
     const long long it = blockIdx.x + (t / TPI) * (long long)gridDim.x;
-    const int chunk = (int)(it % A.nchunks), sl = (int)(it / A.nchunks);
+    const int chunk = (int)(it % A.nchunks);
+    const long long rest = it / A.nchunks;
+    const int sl = (int)(rest % A.nsl), mem = (int)(rest / A.nsl);
     int k = (int)(t % TPI);
     const CUtensorMap* m = &P.tcur;
     int slot = k;
@@ -111,7 +113,8 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
         if (A.need_u0 && m == &P.t1) { if (r == q) m = &P.t0; ++q; }
       }
     }
-    ring.issue_rows(t, m, chunk * W * K::EPC, sl, slot, K::NBOX, K::RB, K::BOX_BYTES);
+    // members follow one another along the x-slice axis of the maps
+    ring.issue_rows(t, m, chunk * W * K::EPC, sl, mem * N, slot, K::NBOX, K::RB, K::BOX_BYTES);
   };
   if (tid == 0) {
     tma_prefetch_desc(&P.tws);
@@ -146,10 +149,12 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
   for (long long k = 0; k < mine; ++k) {  // persistent over work items
     const long long it = blockIdx.x + k * (long long)gridDim.x;
     const int chunk = (int)(it % A.nchunks);
-    const int sl = (int)(it / A.nchunks);
+    const long long rest = it / A.nchunks;
+    const int sl = (int)(rest % A.nsl), mem = (int)(rest / A.nsl);
     const int col = chunk * W + l;
     const bool ok = col < A.nk;
-    const long long base = (long long)sl * A.nkp + col;
+    const long long base = (long long)mem * A.mstride + (long long)sl * A.nkp + col;
+    const double nud = A.mnu ? A.mnu[mem] : A.nu_d;
     auto st = [&](int slot, const C (&v)[V]) {
       if (ok) {
 #pragma unroll
@@ -240,7 +245,7 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
           const C ucm = pu ? pu[T * m * W] : cmk<C>(0, 0);
           const C u0m = p0 ? p0[T * m * W] : ucm;
           const C u1m = p1 ? p1[T * m * W] : cmk<C>(0, 0);
-          v[m] = update_component<Tp, ETD>(A, SC, c, rst[rpos(c, m)], ucm, u0m, u1m, k2, off);
+          v[m] = update_component<Tp, ETD>(A, SC, c, rst[rpos(c, m)], ucm, u0m, u1m, k2, off, nud);
         }
       } else {
 #pragma unroll

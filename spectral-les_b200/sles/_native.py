@@ -29,7 +29,7 @@ EXPORTED = [
     "sles_plan_variant_count", "sles_plan_get_variant", "sles_plan_set_variant", "sles_stage_ctl",
     "sles_plan_check", "sles_selftest_wait_timeout", "sles_selftest_wait_timeout_word", "sles_adjoint_check",
     "sles_static_workspace_check", "sles_static_workspace_selftest_timeout",
-    "sles_plan_set_slab", "sles_slab_info", "sles_slab_buffers", "sles_slab_prime", "sles_slab_middle",
+    "sles_plan_set_slab", "sles_plan_set_batch", "sles_slab_info", "sles_slab_buffers", "sles_slab_prime", "sles_slab_middle",
     "sles_slab_stage",
 ]
 DT_DONE, DT_SNAPSHOT, DT_NAN, DT_TOO_SMALL = 1, 2, 4, 8
@@ -114,6 +114,7 @@ def load_library(path: str = LIB_PATH):
         "sles_plan_get_variant": (i, [vp, i]),
         "sles_plan_set_variant": (i, [vp, i, i]),
         "sles_plan_set_slab": (i, [vp, i, i]),
+        "sles_plan_set_batch": (i, [vp, i, vp, vp]),
         "sles_slab_info": (i, [vp, ctypes.POINTER(SlabLayout)]),
         "sles_slab_buffers": (i, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                   ctypes.POINTER(vp)]),
@@ -150,7 +151,7 @@ def stream_handle(device=None):
 class Plan:
     """Owns a ``sles_plan`` and its workspace (from torch's caching allocator)."""
 
-    def __init__(self, dim, n, dtype, les_model, scheme, parity, nu, cs, forcing, device, slab=None):
+    def __init__(self, dim, n, dtype, les_model, scheme, parity, nu, cs, forcing, device, slab=None, batch=None):
         if not torch.cuda.is_available():
             raise RuntimeError("the spectral-LES B200 path needs a CUDA device; there is no CPU fallback")
         L = load_library()
@@ -163,6 +164,11 @@ class Plan:
         self.h = h
         if slab is not None:  # (nranks, rank): this rank's slab of a decomposed domain
             check(L.sles_plan_set_slab(h, int(slab[0]), int(slab[1])), "sles_plan_set_slab")
+        if batch is not None:  # (nu per member, Cs per member): an ensemble batch of this grid
+            nus, css = batch
+            self.member_nu = torch.tensor([float(x) for x in nus], dtype=torch.float64, device=device)
+            self.member_cs = torch.tensor([float(x) for x in css], dtype=torch.float64, device=device)
+            check(L.sles_plan_set_batch(h, len(nus), ptr(self.member_nu), ptr(self.member_cs)), "sles_plan_set_batch")
         lay = Layout()
         check(L.sles_plan_layout(h, ctypes.byref(lay)), "sles_plan_layout")
         self.hc_elems, self.real_elems, self.nkp, self.nk = lay.hc_elems, lay.real_elems, lay.nkp, lay.nk

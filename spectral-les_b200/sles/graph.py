@@ -18,8 +18,10 @@ from __future__ import annotations
 import torch
 
 from . import ETD2_method, RK3_method, RK4_method
+from . import _native as nat
+from . import autotune
 
-__all__ = ["CapturedStepper", "Ensemble", "PERIOD"]
+__all__ = ["CapturedStepper", "Ensemble", "MemberBatch", "PERIOD"]
 
 PERIOD = 2
 _STEP = {"RK4": RK4_method.solveForNextTimestep, "RK3": RK3_method.solveForNextTimestep,
@@ -37,17 +39,103 @@ def _state_key(d):
     return roles, d._primed, (d.dt, d.nu, d.Cs, d.forcing), d.firstIteration, ctl, d._parity
 
 
-class _Capture:
-    """One CUDA graph advancing several domains by PERIOD steps, each domain
-    on its own captured stream (independent branches of the graph)."""
+class _DomainUnit:
+    """One domain as a unit of a capture: steps through its own plan."""
+
+    def __init__(self, d):
+        self.d = d
+
+    def step(self):
+        _eager_step(self.d)
+
+    def state_key(self):
+        return _state_key(self.d)
+
+    def stepped(self):
+        self.d._mark_stepped()
+
+
+class MemberBatch:
+    """Ensemble members of one grid, dimension, precision, closure, scheme,
+    parity, dt and forcing stepped as one: a batched plan
+    (``sles_plan_set_batch``) runs each pass of every member in one launch,
+    with each member's own viscosity and C_s.  The batch keeps the states in
+    tensors laid out [component][member][...]; ``scatter`` writes them back
+    into the members (the Ensemble does so after every ``advance``).  Every
+    member's first step derives U and curl from its U_hat (a domain stepped
+    alone reuses the physical fields its initial-condition setter stored, which
+    agree to round-off)."""
+
+    @staticmethod
+    def key(d):
+        return (d.dim, d.N, d._rdtype, d.LES_model, d.method, d.parity_mode, float(d.dt), float(d.forcing),
+                str(d.device))
 
     def __init__(self, domains):
-        self.domains = list(domains)
+        self.members = list(domains)
+        d0 = self.members[0]
+        if any(MemberBatch.key(d) != MemberBatch.key(d0) for d in self.members):
+            raise ValueError("a member batch needs one grid, dimension, precision, closure, scheme, parity, dt")
+        if d0.method not in ("RK3", "RK4"):
+            raise ValueError("member batches step RK3 or RK4")
+        les = nat.LES_NONE
+        if d0.LES_ON:
+            les = nat.LES_SMAGORINSKY if d0.LES_model[0] == "S" else nat.LES_VREMAN
+        scheme = nat.SCHEME_RK4 if d0.method == "RK4" else nat.SCHEME_RK3
+        self.plan = nat.Plan(d0.dim, d0.N, d0._rdtype, les, scheme, d0.parity_mode, d0.nu, d0.Cs, d0.forcing,
+                             d0.device, batch=([d.nu for d in self.members], [d.Cs for d in self.members]))
+        autotune.apply_cached(self.plan, d0.method)
+        self.method, self.dt = d0.method, float(d0.dt)
+        shape = (d0.dim, len(self.members)) + tuple(d0._s_uhat.shape[1:])
+        self.A = torch.empty(shape, dtype=d0._s_uhat.dtype, device=d0.device)
+        self.B = torch.zeros_like(self.A)
+        self.C = torch.empty_like(self.A) if self.method == "RK4" else None
+        for b, d in enumerate(self.members):
+            self.A[:, b].copy_(d._s_uhat)
+            if self.C is not None:
+                self.C[:, b].copy_(d._s_u1)
+        self._primed = None
+
+    def step(self):
+        """One step of every member (src/RK4_method.py:20-35 / src/RK3_method.py:20-41)."""
+        A, B, C = self.A, self.B, self.C
+        nst = 4 if self.method == "RK4" else 3
+        base = nat.STAGE_RK4 if self.method == "RK4" else 0
+        for rk in range(nst):
+            ucur = A if rk == 0 else B
+            primed = rk > 0 or self._primed == A.data_ptr()
+            self.plan.stage(rk, self.dt, ucur, A, C, B, None, None, None, base | (nat.STAGE_PRIMED if primed else 0))
+        self.A, self.B = B, A
+        self._primed = B.data_ptr()
+
+    def state_key(self):
+        return (self.A.data_ptr(), self.B.data_ptr(), self._primed)
+
+    def stepped(self):
+        pass
+
+    def scatter(self):
+        """Write the batch's states back into the member domains."""
+        for b, d in enumerate(self.members):
+            d._s_uhat.copy_(self.A[:, b])
+            if self.C is not None:
+                d._s_u1.copy_(self.C[:, b])
+            d._mark_stepped()
+            d._primed = None
+
+
+class _Capture:
+    """One CUDA graph advancing several units (domains or member batches) by
+    PERIOD steps, each unit on its own captured stream (independent branches
+    of the graph)."""
+
+    def __init__(self, domains):
+        self.domains = [u if isinstance(u, (MemberBatch, _DomainUnit)) else _DomainUnit(u) for u in domains]
         self.graph = None
         self.keys = None
 
     def valid(self):
-        return self.graph is not None and [_state_key(d) for d in self.domains] == self.keys
+        return self.graph is not None and [u.state_key() for u in self.domains] == self.keys
 
     def warm_and_capture(self):
         """Run PERIOD eager steps (first-step logic, cached launch attributes,
@@ -55,10 +143,10 @@ class _Capture:
         steps executed on the GPU (PERIOD)."""
         self.graph = None
         for _ in range(PERIOD):
-            for d in self.domains:
-                _eager_step(d)
+            for u in self.domains:
+                u.step()
         torch.cuda.synchronize()
-        before = [_state_key(d) for d in self.domains]
+        before = [u.state_key() for u in self.domains]
         main = torch.cuda.Stream()
         side = [torch.cuda.Stream() for _ in self.domains]
         g = torch.cuda.CUDAGraph()
@@ -67,13 +155,13 @@ class _Capture:
             # the members' launch sequences are independent (concurrent) nodes
             for s in side:
                 s.wait_stream(main)
-            for d, s in zip(self.domains, side):
+            for u, s in zip(self.domains, side):
                 with torch.cuda.stream(s):
                     for _ in range(PERIOD):
-                        _eager_step(d)
+                        u.step()
             for s in side:
                 main.wait_stream(s)
-        after = [_state_key(d) for d in self.domains]
+        after = [u.state_key() for u in self.domains]
         if after != before:
             raise RuntimeError("step state did not return to its start after %d steps" % PERIOD)
         self.graph, self.keys = g, after
@@ -81,8 +169,8 @@ class _Capture:
 
     def replay(self):
         self.graph.replay()
-        for d in self.domains:
-            d._mark_stepped()
+        for u in self.domains:
+            u.stepped()
 
 
 def _advance(cap, nsteps, eager_one):
@@ -114,18 +202,40 @@ class CapturedStepper:
 
 class Ensemble:
     """Independent domains of any grid size, dimension and parameters, stepped
-    together: one graph replay advances every member by PERIOD steps, each
-    member on its own captured stream so small members run concurrently."""
+    together: one graph replay advances every member by PERIOD steps.  With
+    ``batch=True`` (the default) members sharing a grid, dimension, precision,
+    closure, RK scheme, parity, dt and forcing form a MemberBatch (one launch
+    per pass for all of them, each with its own viscosity and C_s); every
+    batch and every remaining member is a branch of the graph on its own
+    captured stream, so they run concurrently."""
 
-    def __init__(self, domains):
+    def __init__(self, domains, batch=True):
         self.members = list(domains)
-        self._c = _Capture(self.members)
+        self.batches = []
+        units = []
+        if batch:
+            groups = {}
+            for d in self.members:
+                groups.setdefault(MemberBatch.key(d), []).append(d)
+            for k, ds in groups.items():
+                if len(ds) > 1 and ds[0].method in ("RK3", "RK4"):
+                    mb = MemberBatch(ds)
+                    self.batches.append(mb)
+                    units.append(mb)
+                else:
+                    units.extend(_DomainUnit(d) for d in ds)
+        else:
+            units = [_DomainUnit(d) for d in self.members]
+        self.units = units
+        self._c = _Capture(units)
 
     def advance(self, nsteps):
         def one():
-            for d in self.members:
-                _eager_step(d)
+            for u in self.units:
+                u.step()
         _advance(self._c, nsteps, one)
+        for mb in self.batches:
+            mb.scatter()
 
     def advance_sequential(self, nsteps):
         """The same steps run member by member without graphs (comparison)."""

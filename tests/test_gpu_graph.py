@@ -65,3 +65,39 @@ def test_ensemble_of_uneven_members_matches_members_alone():
     torch.cuda.synchronize()
     for e, s in zip(ens.members, solo):
         assert _rel(e.U_hat, s.U_hat) < 1e-6
+
+
+def _member(dim, n, dtype, les, method, nu, cs, seed):
+    if dim == 3:
+        d = InitializeDomain(nu=nu, dimension=3, time_stepSize=1e-3, No_of_gridpoint=(4 if les else 1) * n,
+                             method=method, LES_ON=1 if les else 0, LES_model=les, Cs=cs, dtype=dtype)
+        initial_velocity(d, *random_spectrum_velocity(n, 4.0, 1.0, seed=seed))
+    else:
+        d = InitializeDomain(nu=nu, dimension=2, time_stepSize=1e-3, No_of_gridpoint=n, method=method, dtype=dtype)
+        initial_vorticity(d, gaussian_vorticity_2d(n, seed=seed))
+    d.U_hat1[...] = d.U_hat
+    return d
+
+
+@pytest.mark.parametrize("dtype,tol", [("float64", 1e-12), ("float32", 2e-6)])
+def test_member_batches_match_members_alone(dtype, tol):
+    """Members of one grid and scheme run as one batched plan (one launch per
+    pass, each member's own nu and Cs): the same states as stepping each
+    member alone, up to the round-off of the first step (a batch derives U
+    and curl from U_hat where a lone domain reuses its setter's fields)."""
+    spec = [(3, 32, "Smagorinsky", "RK4", 1e-3, 0.12), (3, 32, "Smagorinsky", "RK4", 2e-4, 0.19),
+            (3, 32, "Smagorinsky", "RK4", 5e-4, 0.15), (2, 64, None, "RK4", 1e-5, 0.14),
+            (2, 64, None, "RK4", 3e-4, 0.14), (3, 32, "vreman", "RK3", 1e-3, 0.16), (3, 32, "vreman", "RK3", 3e-3, 0.11),
+            (3, 48, None, "RK4", 1e-3, 0.14)]
+    mk = lambda: [_member(dm, n, dtype, les, me, nu, cs, 20 + i) for i, (dm, n, les, me, nu, cs) in enumerate(spec)]
+    ens = Ensemble(mk(), batch=True)
+    assert len(ens.batches) == 3 and len(ens.units) == 4
+    solo = mk()
+    ens.advance(7)
+    ens.advance(3)
+    for d in solo:
+        for _ in range(10):
+            _eager_step(d)
+    torch.cuda.synchronize()
+    for e, s in zip(ens.members, solo):
+        assert _rel(e.U_hat, s.U_hat) < tol
