@@ -395,8 +395,10 @@ def run_reference(args, rank, world):
     value, secs = cpu_oracle_rate(n, k, w, 0, cores)
     sample = ("%d timed RK3 step(s) at %d^3 after %d warm-up step(s); the rate stands for the requested %d "
               "steps (%.0f s at %.1f s/step, extrapolated); oracle port (NumPy + scipy.fft workers=%d) on the "
-              "host cores; the reference itself needs mpi4py/mpi4py-fft, absent on this image" %
-              (k, n, w, args.steps, secs / k * args.steps, secs / k, cores))
+              "host cores; the reference itself needs mpi4py/mpi4py-fft, absent on this image (its own src/ "
+              "under a single-rank shim with the same threaded FFTs took 0.88x the port's time per step at "
+              "256^3 on an 8-core CPU: oracle/time_reference.py)" % (k, n, w, args.steps, secs / k * args.steps,
+                                                                     secs / k, cores))
     out = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
            "steps": k, "steps_requested": args.steps, "warmup": w, "ms_per_step": round(secs / k * 1e3, 2),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -653,8 +655,10 @@ def bench_ensemble(rank, steps=200):
     out = {"value": round(pts * steps / tg / 1e6, 2), "unit": UNIT, "members": len(a), "steps": steps,
            "points_per_step": pts, "sequential_value": round(pts * steps / ts / 1e6, 2),
            "speedup_vs_sequential": round(ts / tg, 3), "max_member_rel_l2_vs_sequential": max(diffs),
+           "batches": [len(mb.members) for mb in ens.batches], "single_members": len(ens.units) - len(ens.batches),
            "config": "32 2D vorticity (N in {256,512,1024}, RK4) + 16 3D Smagorinsky (N in {64,96,128}, RK4), FP32; "
-                     "graph replay with one stream branch per member vs members one at a time"}
+                     "members of one grid and scheme batched into one plan (one launch per pass, per-member nu and "
+                     "Cs), batches and single members as branches of one replayed graph, vs members one at a time"}
     del a, b, ens, seq
     torch.cuda.empty_cache()
     return out
