@@ -664,6 +664,108 @@ def bench_ensemble(rank, steps=200):
     return out
 
 
+def bench_zoo(rank):
+    """One short run of every kind of kernel the library launches (for an ncu
+    capture of each kernel's first launch): the 3D fused passes at 256^3 FP32
+    (Smagorinsky RK3 on every x variant, Vreman corrected ETD2, no-LES RK4,
+    the alternative y/z variants), the FP64 passes, the 2D passes at 1024^2,
+    the standalone transforms and diagnostics, the device-dt controller, the
+    adjoint passes at 64^3, a slab decomposition and a member batch."""
+    import torch
+    from sles import ETD2_method, RK3_method, RK4_method, diagnostics
+    from sles import _native as nat
+    from sles.adjoint import RK4Rollout
+    from sles.graph import MemberBatch
+    from sles.initial import initial_vorticity
+    from sles.initialize_domain import InitializeDomain
+    from sles.slab import SlabDomain, emulated_exchange
+    from sles.synthetic import gaussian_vorticity_2d
+    done = []
+
+    def release():
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
+    d = make_domain(256, "float32", rank)
+    for v in range(4):
+        d._plan.set_variant(v, nat.PASS_X)
+        RK3_method.solveForNextTimestep(d)
+    d._plan.set_variant(3, nat.PASS_X)
+    for py, pz in ((1, 0), (0, 1)):
+        d._plan.set_variant(py, nat.PASS_Y)
+        d._plan.set_variant(pz, nat.PASS_Z)
+        RK3_method.solveForNextTimestep(d)
+    diagnostics.diag(d, with_max=True, nshell=200)
+    U = d.U
+    del d, U
+    release()
+    done.append("256^3 f32 smag rk3 (x variants 0-3, y/z variants), diag, c2r")
+    d = make_domain(256, "float32", rank, method="ETD2", les="vreman", nu=5e-5, cs=math.sqrt(0.028), dt=5e-4,
+                    k0=6.0, parity=False)
+    for _ in range(2):
+        ETD2_method.solveForNextTimestep(d)
+    del d
+    release()
+    d = make_domain(256, "float32", rank, method="RK4", les=None)
+    d.U_hat1[...] = d.U_hat
+    RK4_method.solveForNextTimestep(d)
+    del d
+    release()
+    d = make_domain(128, "float64", rank)
+    RK3_method.solveForNextTimestep(d)
+    del d
+    release()
+    done.append("256^3 vreman etd2, 256^3 no-LES rk4, 128^3 f64")
+    for les in (None, "Smagorinsky"):
+        d2 = InitializeDomain(nu=1e-4, dimension=2, time_stepSize=1e-3, No_of_gridpoint=(4 if les else 1) * 1024,
+                              method="RK4", LES_ON=1 if les else 0, LES_model=les, Cs=0.17, dtype="float32")
+        initial_vorticity(d2, gaussian_vorticity_2d(1024, seed=rank))
+        d2.U_hat1[...] = d2.U_hat
+        RK4_method.solveForNextTimestep(d2)
+        del d2
+        release()
+    done.append("2D 1024^2 rk4 (no LES, Smagorinsky)")
+    from sles.SM_solver import spectralMethodSolver
+    import tempfile
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as td:
+        os.chdir(td)
+        try:
+            d = make_domain(64, "float32", rank)
+            d.T = 0.02
+            spectralMethodSolver(d, No_Ek_plot=1, verbose=False, device_dt=True, chunk=4)
+        finally:
+            os.chdir(cwd)
+    del d
+    release()
+    done.append("device-dt controller at 64^3")
+    ro = RK4Rollout(64, 1e-3, 1e-3, les="Smagorinsky", Cs=0.17, dtype=torch.float32, checkpoint_every=2)
+    U0 = make_domain(64, "float32", rank, method="RK4").U_hat.clone().to(ro.cdtype)
+    UT, ck = ro.forward_states(U0, 0.17, 2)
+    ro.backward_states(ck, UT[..., : ro.nk].clone(), 0.17, 2)
+    del ro, U0, UT, ck
+    release()
+    done.append("adjoint rk4 at 64^3")
+    base = make_domain(256, "float32", rank)
+    doms = [SlabDomain(256, nu=NU, dt=DT, method="RK3", les="Smagorinsky", Cs=CS, dtype=torch.float32, nranks=2,
+                       rank=r, exchange=lambda o, i: None) for r in range(2)]
+    for sd in doms:
+        sd.set_state(base.U_hat)
+    emulated_exchange(doms)()
+    del doms, base
+    release()
+    done.append("slab P=2 at 256^3")
+    ms = [make_domain(128, "float32", rank + i, method="RK4", cs=0.12 + 0.02 * i) for i in range(3)]
+    for m in ms:
+        m.U_hat1[...] = m.U_hat
+    mb = MemberBatch(ms)
+    mb.step()
+    del mb, ms
+    release()
+    done.append("member batch of 3 at 128^3")
+    return {"ran": done}
+
+
 def bench_kernels(case, n, precision, rank, xvar=-1):
     """Mean ms per launch of each kernel class of one RHS evaluation
     (sles_profile_rhs, CUDA events, 20 evaluations) and its algorithmic GB/s."""
@@ -759,7 +861,7 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (use the default or cached kernel variants)")
-    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble", "driver", "fft", "steps", "kernels"],
+    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble", "driver", "fft", "steps", "kernels", "zoo"],
                     help="run one extra block alone and print it (profiling; not a bench line); 'steps': "
                          "--case at --n stepped --steps times after --warmup (for ncu launch lists)")
     ap.add_argument("--case", default="smag_rk3", choices=["smag_rk3", "vreman_etd2", "smag_rk4"],
@@ -803,6 +905,7 @@ def main():
               "ensemble": lambda: bench_ensemble(rank), "driver": lambda: bench_driver(rank),
               "fft": lambda: bench_fft(rank),
               "kernels": lambda: bench_kernels(args.case, args.n, args.precision, rank, args.xvar),
+              "zoo": lambda: bench_zoo(rank),
               "steps": lambda: bench_steps(args.case, args.n, args.precision, args.steps, args.warmup, rank,
                                            args.xvar)}[args.only]
         print(json.dumps({"only": args.only, "result": fn()}))
