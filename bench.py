@@ -170,6 +170,76 @@ def spectrum_error(a, b, n, floor=1e-8):
     return float(r[live].max()), klast, float(r.max())
 
 
+def error_history(d32, d64, step, nsteps, n, every=None):
+    """Step both domains ``nsteps`` times, recording after every step the
+    relative L2 velocity error of the float32 state against the float64 one
+    and the E(k) error (shells above 1e-8 of the peak).  Returns the maxima,
+    the final values and a thinned series."""
+    every = every or max(1, nsteps // 10)
+    l2, ek = [], []
+    for _ in range(nsteps):
+        step(d32)
+        step(d64)
+        l2.append(rel_l2(d32.U_hat, d64.U_hat))
+        ek.append(spectrum_error(d32.U_hat, d64.U_hat, n)[0])
+    return {"steps": nsteps, "rel_l2_max": max(l2), "rel_l2_final": l2[-1], "ek_err_max": max(ek),
+            "ek_err_final": ek[-1], "rel_l2_every_%d" % every: [float("%.3g" % x) for x in l2[every - 1::every]],
+            "ek_err_every_%d" % every: [float("%.3g" % x) for x in ek[every - 1::every]]}
+
+
+def bench_cfg2_history(rank, steps=500):
+    """The Smagorinsky LES workload at 256^3 (reference RK3, dt = 1e-3) run
+    for its 500 steps in float32 and in float64 (the oracle precision), with
+    the velocity and E(k) errors recorded after every step."""
+    import torch
+    from sles import RK3_method
+    d32 = make_domain(256, "float32", rank)
+    d64 = make_domain(256, "float64", rank)
+    out = error_history(d32, d64, RK3_method.solveForNextTimestep, steps, 256, every=50)
+    d32._plan.check()
+    d64._plan.check()
+    del d32, d64
+    torch.cuda.empty_cache()
+    out["config"] = "256^3 Smagorinsky Cs=0.17, nu=1e-4, reference RK3, dt=1e-3, seed = rank; float32 vs float64 fused"
+    return out
+
+
+def bench_cfg1(rank):
+    """The plain Taylor-Green case: 64^3, nu = 1/1600, RK4, dt = 0.01, 200
+    steps, float64, no LES; kinetic energy and dissipation every step (the
+    reference's U_square / dissipation_rate outputs, here as E = 1/2 <u.u>
+    and eps = nu <|grad u|^2>).  Reports the rate, E(t) against the analytic
+    early decay 1/8 exp(-6 nu t) over t <= 0.2, and the energy budget
+    dE/dt + eps relative to eps."""
+    import numpy as np
+    import torch
+    from sles import RK4_method, diagnostics
+    from sles.initial import initial_velocity
+    from sles.initialize_domain import InitializeDomain
+    from sles.synthetic import taylor_green
+    n, nu, dt, steps = 64, 1.0 / 1600.0, 0.01, 200
+    d = InitializeDomain(nu=nu, dimension=3, time_stepSize=dt, No_of_gridpoint=n, method="RK4", dtype="float64")
+    initial_velocity(d, *taylor_green(n))
+    d.U_hat1[...] = d.U_hat
+    E, eps = [diagnostics.energy(d)], [diagnostics.dissipation(d)]
+    secs = 0.0
+    for _ in range(steps):
+        secs += time_steps(d, 1, RK4_method.solveForNextTimestep)
+        E.append(diagnostics.energy(d))
+        eps.append(diagnostics.dissipation(d))
+    d._plan.check()
+    E, eps = np.array(E), np.array(eps)
+    t = np.arange(steps + 1) * dt
+    early = t <= 0.2 + 1e-12
+    exact = 0.125 * np.exp(-6 * nu * t)
+    budget = np.abs((E[2:] - E[:-2]) / (2 * dt) + eps[1:-1]) / eps[1:-1]
+    return {"value": round(float(n) ** 3 * steps / secs / 1e6, 2), "unit": UNIT, "steps": steps,
+            "E_0": E[0], "E_end": E[-1], "eps_0": eps[0], "eps_end": eps[-1],
+            "E_rel_dev_from_exp_decay_t_le_0.2": float(np.max(np.abs(E[early] - exact[early]) / exact[early])),
+            "energy_budget_rel_err_max": float(budget.max()),
+            "config": "Taylor-Green 64^3, nu=1/1600, RK4, dt=0.01, 200 steps, float64, no LES; E and eps every step"}
+
+
 def tune_domain(d):
     """Run the autotuner on a domain (outside any timed region); the cache goes
     to a per-process temporary file unless SLES_TUNE_CACHE is set."""
@@ -208,9 +278,7 @@ def bench_512(peak, rank):
         step(d64)
     t32 = time_steps(d32, 20, step)
     t64 = time_steps(d64, 20, step)
-    for _ in range(100 - 23):
-        step(d32)
-        step(d64)
+    hist = error_history(d32, d64, step, 100 - 23, n)
     err = rel_l2(d32.U_hat, d64.U_hat)
     ek, klive, ekall = spectrum_error(d32.U_hat, d64.U_hat, n)
     kms = d32._plan.profile_rhs(d32._s_uhat, d32._new_hc(3), 10)
@@ -231,6 +299,7 @@ def bench_512(peak, rank):
         "rel_l2_fp32_vs_fp64_after_100_steps": err,
         "ek_err_fp32_vs_fp64_after_100_steps": {"max_rel_shells_above_1e-8_of_peak": ek, "up_to_shell": klive,
                                                 "max_rel_all_shells": ekall},
+        "error_every_step_24_to_100": hist,
         "step_roofline_frac": round(STEP_BYTES_PER_PT_RHS["f32"] * 3 * npts / (ms * 1e-3) / 1e9 / peak, 4),
         "kernel_ms": dict(zip(names, [round(x, 4) for x in kms])),
         "kernel_gbs": {k: round(algb[k] / (t * 1e-3) / 1e9, 1) for k, t in zip(names, kms)},
@@ -248,9 +317,7 @@ def bench_512(peak, rank):
         estep(d64)
     t32 = time_steps(d32, 20, estep)
     t64 = time_steps(d64, 20, estep)
-    for _ in range(100 - 23):
-        estep(d32)
-        estep(d64)
+    hist = error_history(d32, d64, estep, 100 - 23, n)
     err = rel_l2(d32.U_hat, d64.U_hat)
     ek, klive, ekall = spectrum_error(d32.U_hat, d64.U_hat, n)
     kms = d32._plan.profile_rhs(d32._s_uhat, d32._new_hc(3), 10)
@@ -267,6 +334,7 @@ def bench_512(peak, rank):
         "rel_l2_fp32_vs_fp64_after_100_steps": err,
         "ek_err_fp32_vs_fp64_after_100_steps": {"max_rel_shells_above_1e-8_of_peak": ek, "up_to_shell": klive,
                                                 "max_rel_all_shells": ekall},
+        "error_every_step_24_to_100": hist,
         "step_roofline_frac": round(STEP_BYTES_PER_PT_RHS["f32"] * 1 * npts / (ms * 1e-3) / 1e9 / peak, 4),
         "kernel_ms": dict(zip(names, [round(x, 4) for x in kms])),
         "kernel_gbs": {k: round(algb[k] / (t * 1e-3) / 1e9, 1) for k, t in zip(names, kms)},
@@ -839,6 +907,9 @@ def north_star_summary(out):
                                "step_model_frac": a["step_roofline_frac"], "kernel_gbs": a.get("kernel_gbs")}
         ns["n512_vreman_etd2"] = {"value": b["value"], "rel_l2_100": r(b["rel_l2_fp32_vs_fp64_after_100_steps"], 10),
                                   "step_model_frac": b["step_roofline_frac"]}
+    if "cfg2_error_history" in out:
+        h = out["cfg2_error_history"]
+        ns["cfg2_500_steps"] = {"rel_l2_max": r(h["rel_l2_max"], 10), "ek_err_max": r(h["ek_err_max"], 8)}
     if "adjoint" in out:
         ns["adjoint_fwd_ratio"] = out["adjoint"]["adjoint_fwd_ratio"]
         ns["adjoint_cs_rel_err"] = r(out["adjoint"]["cs_rel_err_f64_vs_richardson"], 12)
@@ -861,7 +932,8 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (use the default or cached kernel variants)")
-    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble", "driver", "fft", "steps", "kernels", "zoo"],
+    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble", "driver", "fft", "steps", "kernels", "zoo",
+                                       "cfg2"],
                     help="run one extra block alone and print it (profiling; not a bench line); 'steps': "
                          "--case at --n stepped --steps times after --warmup (for ncu launch lists)")
     ap.add_argument("--case", default="smag_rk3", choices=["smag_rk3", "vreman_etd2", "smag_rk4"],
@@ -906,6 +978,7 @@ def main():
               "fft": lambda: bench_fft(rank),
               "kernels": lambda: bench_kernels(args.case, args.n, args.precision, rank, args.xvar),
               "zoo": lambda: bench_zoo(rank),
+              "cfg2": lambda: bench_cfg2_history(rank),
               "steps": lambda: bench_steps(args.case, args.n, args.precision, args.steps, args.warmup, rank,
                                            args.xvar)}[args.only]
         print(json.dumps({"only": args.only, "result": fn()}))
@@ -1025,6 +1098,8 @@ def main():
                                                "max_rel_all_shells": ekall},
                        "note": "FP32 fused vs FP64 fused (same kernels, float64) on the same seeded field"}
     if not args.no_compare and world == 1:
+        out["cfg1_taylor_green"] = bench_cfg1(rank)
+        out["cfg2_error_history"] = bench_cfg2_history(rank)
         out["fft_vs_cufft"] = bench_fft(rank)
         out["n512"] = bench_512(peak, rank)
         adj = bench_adjoint(rank)
