@@ -89,10 +89,14 @@ int sles_plan_layout(const sles_plan* plan, sles_layout* out);
  *   SLES_PASS_Y: the y passes (tile width 8 or 16 columns; variant 1 only for
  *                the float32 3D grids 128, 256, 512, where the count is 2)
  *   SLES_PASS_Z: the fused z pass (1 or 2 z lines per work item; idem)
+ *   SLES_PASS_AX: the adjoint's x pass (sles_adjoint_stage / _prime): 0 direct
+ *                loads, 1 the TMA tile ring for the Runge-Kutta schemes (the
+ *                3D grids 128, 256, 512, where the count is 2 and 1 is the
+ *                default; ETD2 reverse steps load directly under either)
  * sles_plan_variant_count returns 0 for an invalid pass (1: no alternative);
  * sles_plan_get_variant returns -1 for an invalid pass.
  */
-enum { SLES_PASS_X = 0, SLES_PASS_Y = 1, SLES_PASS_Z = 2 };
+enum { SLES_PASS_X = 0, SLES_PASS_Y = 1, SLES_PASS_Z = 2, SLES_PASS_AX = 3 };
 int sles_plan_variant_count(const sles_plan* plan, int pass);
 int sles_plan_get_variant(const sles_plan* plan, int pass);
 int sles_plan_set_variant(sles_plan* plan, int pass, int variant);

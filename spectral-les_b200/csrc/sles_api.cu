@@ -82,6 +82,7 @@ int sles_plan_create(const sles_plan_desc* d, sles_plan** out) {
   I.scal = nullptr;
   I.xvar = eng->default_xvar();
   I.yvar = I.zvar = 0;
+  I.axvar = eng->variant_count(SLES_PASS_AX) - 1;
   I.slab_p = 1;
   I.slab_r = 0;
   I.slab_m = d->n;
@@ -150,6 +151,7 @@ int sles_plan_get_variant(const sles_plan* p, int pass) {
     case SLES_PASS_X: return p->info.xvar;
     case SLES_PASS_Y: return p->info.yvar;
     case SLES_PASS_Z: return p->info.zvar;
+    case SLES_PASS_AX: return p->info.axvar;
     default: return -1;
   }
 }
@@ -161,6 +163,7 @@ int sles_plan_set_variant(sles_plan* p, int pass, int variant) {
     case SLES_PASS_X: p->info.xvar = variant; break;
     case SLES_PASS_Y: p->info.yvar = variant; break;
     case SLES_PASS_Z: p->info.zvar = variant; break;
+    case SLES_PASS_AX: p->info.axvar = variant; break;
     default: return SLES_ERR_INVALID_ARG;
   }
   return SLES_OK;

@@ -44,6 +44,7 @@ class DtCtl(ctypes.Structure):
                 ("nsteps", ctypes.c_uint32), ("t_init", ctypes.c_uint32), ("resumed", ctypes.c_uint32),
                 ("reserved", ctypes.c_uint32)]
 PASS_X, PASS_Y, PASS_Z = 0, 1, 2
+PASS_AX = 3  # the adjoint x pass (not timed by the forward autotuner)
 PASSES = (PASS_X, PASS_Y, PASS_Z)
 
 

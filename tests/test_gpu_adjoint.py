@@ -47,7 +47,18 @@ _UNSUPPORTED = 2  # SLES_ERR_UNSUPPORTED, include/sles.h
 @pytest.mark.parametrize("method", ["RK4", "RK3", "SSP3"])
 @pytest.mark.parametrize("les", ["Smagorinsky", "vreman", None])
 def test_one_step_vjp_matches_torch_autograd(les, method):
-    n, nu, dt, cs = 32, 3e-3, 5e-3, 0.17
+    _one_step_vjp(32, 3e-3, 5e-3, 0.17, les, method)
+
+
+def test_one_step_vjp_256_matches_torch_autograd():
+    """The adjoint z pass on the 256-point grid's z-line plan (128-point
+    half-length transforms pairing each bin with its mirror in one thread):
+    one RK4 Smagorinsky step, float64."""
+    _one_step_vjp(256, 1e-4, 1e-3, 0.17, "Smagorinsky", "RK4")
+    torch.cuda.empty_cache()
+
+
+def _one_step_vjp(n, nu, dt, cs, les, method):
     ro, ps = _pair(method, n, nu, dt, les, cs, 1)
     step = ps.rk4 if method == "RK4" else ps.rk3
     U0 = ps.rfft(_field(n))
@@ -212,3 +223,36 @@ def test_schemes_without_an_adjoint_are_refused(scheme, parity):
         plan.adjoint_stage(ws, 0, 1e-3, None, z, z.clone(), z.clone(), csg)
     assert e.value.status == _UNSUPPORTED
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("method", ["RK4", "RK3", "SSP3", "ETD2"])
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-11), (torch.float32, 1e-4)])
+def test_adjoint_x_pass_forms_agree(method, dtype, tol):
+    # ETD2: the reverse ETD2 steps load directly under both settings; its first
+    # (RK4) step's reverse runs on the companion RK4 plan, which does switch
+    """The adjoint x pass through the TMA tile ring (SLES_PASS_AX variant 1, the
+    default) against the direct-load form (variant 0): same reverse sweep,
+    128^3, 3 steps with checkpoints every 2 (prime, interior and last stages)."""
+    n, nu, dt, cs, steps = 128, 1e-3, 2e-3, 0.17, 3
+    if method == "ETD2":
+        ro = ETD2Rollout(n, nu, dt, les="Smagorinsky", Cs=cs, dtype=dtype, checkpoint_every=2)
+        plans = (ro.plan, ro.rk.plan)
+    else:
+        ro = _ROLLOUT[method](n, nu, dt, les="Smagorinsky", Cs=cs, dtype=dtype, parity=method != "SSP3",
+                              checkpoint_every=2)
+        plans = (ro.plan,)
+    for p in plans:
+        assert p.variant_count(nat.PASS_AX) == 2 and p.get_variant(nat.PASS_AX) == 1
+    U0 = ro.rfft(_field(n, seed=5))
+    UT, ck = ro.forward_states(U0, cs, steps)
+    g0 = torch.randn(UT[..., : ro.nk].shape, dtype=ro.rdtype, device="cuda",
+                     generator=torch.Generator(device="cuda").manual_seed(1)).to(ro.cdtype)
+    out = []
+    for v in (0, 1):
+        for p in plans:
+            p.set_variant(v, nat.PASS_AX)
+        g, c = ro.backward_states(ck, g0, cs, steps)
+        out.append((g[..., : ro.nk].to(torch.complex128).clone(), float(c)))
+    (ga, ca), (gb, cb) = out
+    assert _rel(gb, ga) < tol
+    assert abs(cb - ca) <= tol * abs(ca)
