@@ -279,7 +279,7 @@ struct AZArgs {
 
 template <typename Tp, int N, int LPI>
 struct AZGeo {
-  using F = typename PlanFor<Tp, N / 2>::F;
+  using F = typename MirrorIf<typename PlanFor<Tp, N / 2>::F>::type;  // as the forward z pass
   using C = typename CT<Tp>::C;
   static constexpr int L = N / 2, T = F::T, V = F::V;
   static constexpr int NGT = 12;                  // thread groups
@@ -468,7 +468,7 @@ k_adj_zpass(const AZArgs<Tp> A) {
       F::template lsync<WS>();
       const Tp sc = r == 0 ? A.scale : (Tp)1;
 #pragma unroll
-      for (int m = 0; m < V; ++m) sm[j + T * m] = cscale(v[m], sc);
+      for (int m = 0; m < V; ++m) sm[F::pos(j, m)] = cscale(v[m], sc);
     }
     __syncthreads();
     // ---- phase B: pointwise adjoint
@@ -488,7 +488,8 @@ k_adj_zpass(const AZArgs<Tp> A) {
 #pragma unroll
       for (int m = 0; m < V; ++m) v[m] = sm[j + T * m];
       fft.template run<-1, WS>(v, j, sm, 1);
-      r2c_post<F, WS>(v, j, sm, 1, twN, [&](int k, C x) { spec[k] = x; });
+      if constexpr (F::MIR) r2c_post_mir<F>(v, j, twN, [&](int k, C x) { spec[k] = x; });
+      else r2c_post<F, WS>(v, j, sm, 1, twN, [&](int k, C x) { spec[k] = x; });
     }
     __syncthreads();
     // ---- phase D: Z_c = ubar_c - i kz abar_3c, A1_c, A2_c with weights w/N^3

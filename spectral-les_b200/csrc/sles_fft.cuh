@@ -166,7 +166,11 @@ struct LineFFT {
   static constexpr int TW1 = (S >= 2) ? NB1 * (R1 - 1) : 1;
   static constexpr int TW2 = (S >= 3) ? NB2 * (R2 - 1) : 1;
   static constexpr int PADD = PADD_ > 0 ? PADD_ : R0;
+  static constexpr int RAD0 = R0, RAD1 = R1, RAD2 = R2;
   static constexpr int XLEN = L + L / PADD + 1;  // exchange line length (slots)
+  // output bin of register m of thread j (the cyclic distribution)
+  static constexpr bool MIR = false;
+  __device__ __forceinline__ static int pos(int j, int m) { return j + T * m; }
   __device__ __forceinline__ static int pad(int p) { return p + (int)((unsigned)p / (unsigned)PADD); }
   // per-stage twiddle tables, [r][k] so a warp reads consecutive entries:
   // stage 1: W_{R0 R1}^{k r}, k < R0; stage 2: W_L^{k r}, k < R0 R1
@@ -364,6 +368,55 @@ struct WithPad<LineFFT<Tp, L, R0, R1, R2, T, P0>, P> {
   using F = LineFFT<Tp, L, R0, R1, R2, T, P>;
 };
 
+// The plan with the second butterfly of its last stage mirrored: thread j runs
+// the last-stage butterflies j and 2T - j (thread 0: 0 and T) in place of j
+// and j + T, so its outputs are the bins b_q + 2T r (q = register m mod 2,
+// r = m / 2) and every bin k has its mirror L - k in the same thread: the
+// real<->half-complex post step (r2c_post_mir) needs no exchange.  For plans
+// of two stages with two last-stage butterflies per thread (R0 = 2T).  Inputs
+// stay cyclic; only the outputs are permuted (pos).
+template <class B>
+struct MirrorFFT : B {
+  using C = typename B::C;
+  using Tp = decltype(C::x);
+  static constexpr int L = B::L, T = B::T, V = B::V, R0 = B::RAD0, R1 = B::RAD1;
+  static_assert(B::S == 2 && B::NB1 == 2 && R0 == 2 * T, "mirrored plans have two stages, two last butterflies");
+  static constexpr bool MIR = true;
+  __device__ __forceinline__ static int bfly1(int j) { return j ? 2 * T - j : T; }
+  __device__ __forceinline__ static int pos(int j, int m) { return ((m & 1) ? bfly1(j) : j) + R0 * (m >> 1); }
+  // register holding the mirror bin (L - k) mod L of register m (j != 0, j == 0)
+  static constexpr int mirror_reg(int m, bool j0) {
+    return !j0 ? (1 - (m & 1)) + 2 * (R1 - 1 - (m >> 1))
+               : ((m & 1) ? 1 + 2 * (R1 - 1 - (m >> 1)) : ((m >> 1) == 0 ? 0 : 2 * (R1 - (m >> 1))));
+  }
+  __device__ __forceinline__ void init(int j) {
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int k = q ? bfly1(j) : j;  // < R0
+#pragma unroll
+      for (int r = 1; r < R1; ++r) this->tw1[q * (R1 - 1) + r - 1] = twiddle<Tp>((long long)k * r, R0 * R1, -1);
+    }
+  }
+  template <int DIR, int WS = 0>
+  __device__ __forceinline__ void run(C (&v)[V], int j, C* sm, int ws) {
+    B::template lsync<WS>();
+    this->template stage<R0, DIR, false, false>(v, this->tw1, 1, j, sm, ws);
+    B::template lsync<WS>();
+    const int b1 = bfly1(j);
+#pragma unroll
+    for (int m = 0; m < V; ++m) v[m] = sm[B::pad(((m & 1) ? b1 : j) + R0 * (m >> 1)) * ws];
+    this->template stage<R1, DIR, true, true>(v, this->tw1, R0, j, sm, ws);
+  }
+};
+
+// MirrorFFT<F> where F qualifies (and SLES_MIRROR != 0), else F
+#ifndef SLES_MIRROR
+#define SLES_MIRROR 1
+#endif
+template <class F, bool OK = (SLES_MIRROR != 0 && F::S == 2 && F::NB1 == 2 && F::RAD0 == 2 * F::T)>
+struct MirrorIf { using type = F; };
+template <class F> struct MirrorIf<F, true> { using type = MirrorFFT<F>; };
+
 // Plans with at most 8-12 points per thread, for passes that keep several
 // transformed lines live in registers at once (one more exchange per line).
 template <typename Tp, int L> struct PlanLo { using F = typename PlanFor<Tp, L>::F; };
@@ -415,6 +468,26 @@ __device__ __forceinline__ void r2c_post(typename F::C (&v)[F::V], int j, typena
     C t = cmulmi(cmul(twN[k], d));
     out(k, cmk<C>((Tp)0.5 * (s.x + t.x), (Tp)0.5 * (s.y + t.y)));
     if (k == 0) out(F::L, cmk<C>(z.x - z.y, (Tp)0));
+  }
+}
+
+// r2c post-processing on a mirrored plan's outputs (MirrorFFT): each bin's
+// mirror is in the thread's own registers, so no exchange and no barrier.
+// Emits out(k, X_k) for the thread's bins (k = F::pos(j, m)) and bin L by j == 0.
+template <class F, class Dst>
+__device__ __forceinline__ void r2c_post_mir(typename F::C (&v)[F::V], int j, const typename F::C* twN, Dst out) {
+  using C = typename F::C;
+  using Tp = decltype(C::x);
+  const bool j0 = (j == 0);
+#pragma unroll
+  for (int m = 0; m < F::V; ++m) {
+    const int k = F::pos(j, m);
+    const C z = v[m];
+    const C zc = cconj(j0 ? v[F::mirror_reg(m, true)] : v[F::mirror_reg(m, false)]);
+    C s = cadd(z, zc), d = csub(z, zc);
+    C t = cmulmi(cmul(twN[k], d));
+    out(k, cmk<C>((Tp)0.5 * (s.x + t.x), (Tp)0.5 * (s.y + t.y)));
+    if (m == 0 && j0) out(F::L, cmk<C>(z.x - z.y, (Tp)0));
   }
 }
 

@@ -74,7 +74,7 @@ k_c2c_axis(const typename CT<Tp>::C* src, typename CT<Tp>::C* dst,  // may alias
 // ---------------------------------------------------------------------------
 template <typename Tp, int NR, int LPB>
 struct RealAxis {
-  using F = typename PlanFor<Tp, NR / 2>::F;
+  using F = typename MirrorIf<typename PlanFor<Tp, NR / 2>::F>::type;  // mirrored where the plan allows
   using C = typename CT<Tp>::C;
   static constexpr int L = NR / 2;
   static constexpr int T = F::T;
@@ -108,9 +108,15 @@ k_r2c_line(const Tp* __restrict__ src, typename CT<Tp>::C* __restrict__ dst, lon
 #pragma unroll
     for (int m = 0; m < K::F::V; ++m) v[m] = ok ? in[j + K::T * m] : cmk<C>(0, 0);
     fft.template run<-1, K::WS>(v, j, scr + ln * K::LS, 1);
-    r2c_post<typename K::F, K::WS>(v, j, scr + ln * K::LS, 1, twN, [&](int k, C x) {
-      if (ok) out[k] = x;
-    });
+    if constexpr (K::F::MIR) {
+      r2c_post_mir<typename K::F>(v, j, twN, [&](int k, C x) {
+        if (ok) out[k] = x;
+      });
+    } else {
+      r2c_post<typename K::F, K::WS>(v, j, scr + ln * K::LS, 1, twN, [&](int k, C x) {
+        if (ok) out[k] = x;
+      });
+    }
   }
 }
 
@@ -140,7 +146,7 @@ k_c2r_line(const typename CT<Tp>::C* __restrict__ src, Tp* __restrict__ dst, lon
     fft.template run<+1, K::WS>(v, j, scr + ln * K::LS, 1);
     if (ok) {
 #pragma unroll
-      for (int m = 0; m < K::F::V; ++m) out[j + K::T * m] = cscale(v[m], scale);
+      for (int m = 0; m < K::F::V; ++m) out[K::F::pos(j, m)] = cscale(v[m], scale);
     }
   }
 }

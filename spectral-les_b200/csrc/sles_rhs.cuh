@@ -829,7 +829,9 @@ static __global__ void k_dtctl(sles_dtctl* c, int parity) {
 #endif
 template <typename Tp, int N, int DIM, int LES, int PAR2D, int LPI>
 struct ZGeo {
-  using F = typename WithPad<typename PlanFor<Tp, N / 2>::F, SLES_Z_PADD>::F;
+  // the half-length plan, mirrored where it qualifies (the r2c post step
+  // then pairs bins in registers)
+  using F = typename MirrorIf<typename WithPad<typename PlanFor<Tp, N / 2>::F, SLES_Z_PADD>::F>::type;
   using C = typename CT<Tp>::C;
   static constexpr int L = N / 2, T = F::T, V = F::V;
   static constexpr int NG = (DIM == 3) ? (LES ? 12 : 6) : (LES ? 6 : 3);    // physical fields
@@ -1033,7 +1035,7 @@ k_zpass(const ZArgs<Tp> A) {
       F::template lsync<WS>();  // the region doubles as exchange scratch: all reads done
       C* dst = reinterpret_cast<C*>(myreg);
 #pragma unroll
-      for (int m = 0; m < V; ++m) dst[j + T * m] = cscale(v[m], A.scale);
+      for (int m = 0; m < V; ++m) dst[F::pos(j, m)] = cscale(v[m], A.scale);
     }
     __syncthreads();
     // ---- phase B: pointwise products
@@ -1082,9 +1084,15 @@ k_zpass(const ZArgs<Tp> A) {
       fft.template run<-1, WS>(v, j, sm, 1);
       C* out = A.ws + (grp < K::NOUT ? grp : 0) * fs + lo;
       const bool wr = ok && grp < K::NOUT;
-      r2c_post<F, WS>(v, j, sm, 1, twN, [&](int k, C x) {
-        if (wr) out[k] = x;
-      });
+      if constexpr (F::MIR) {
+        r2c_post_mir<F>(v, j, twN, [&](int k, C x) {
+          if (wr) out[k] = x;
+        });
+      } else {
+        r2c_post<F, WS>(v, j, sm, 1, twN, [&](int k, C x) {
+          if (wr) out[k] = x;
+        });
+      }
     }
   }
   if (A.umax) {  // block maximum through the (now idle) line regions, one atomic per block

@@ -52,7 +52,10 @@ def random_spectrum_velocity(n, k0=4.0, u0=1.0, seed=0, device="cuda"):
     w = torch.where((kz > 0) & (kz < n // 2), 2.0, 1.0)
     shell = torch.round(kmag).to(torch.int64).expand(uh.shape[1:])
     e_mode = (0.5 * torch.sum(uh.real ** 2 + uh.imag ** 2, 0) * w).reshape(-1)
-    e_shell = torch.bincount(shell.reshape(-1), weights=e_mode)
+    # shell sums on the host: bincount with weights is sequential there (on the
+    # GPU it accumulates with atomics, whose order, and so the last bits of
+    # every field made from it, changes from call to call)
+    e_shell = torch.bincount(shell.reshape(-1).cpu(), weights=e_mode.cpu()).to(device)
     target = _model_spectrum(torch.arange(e_shell.numel(), device=device, dtype=torch.float64), k0, u0)
     scale = torch.where(e_shell > 0, torch.sqrt(target / torch.where(e_shell > 0, e_shell, torch.ones_like(e_shell))),
                         torch.zeros_like(e_shell))

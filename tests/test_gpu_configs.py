@@ -105,3 +105,35 @@ def test_fused_against_plain_torch_fp64(n):
     del d32, Uh, ps
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("dim,les", [(3, None), (2, "Smagorinsky"), (2, None)])
+def test_fused_256_other_forms_against_plain_torch_fp64(dim, les):
+    """The 256-point grid's z-line plan (128-point half-length transforms whose
+    last stage pairs each bin with its mirror in one thread) in the pass forms
+    the Smagorinsky recipe above does not run: 3D without LES and 2D with and
+    without Smagorinsky, RK4, float64, 3 steps against the plain torch.fft path
+    (relative L2 below 1e-11; 2D LES in the corrected stress form, which the
+    plain path implements)."""
+    from sles.initial import initial_vorticity
+    from sles.synthetic import gaussian_vorticity_2d
+    n, steps = 256, 3
+    nu = 1e-4 if dim == 3 else 1e-3
+    d = InitializeDomain(nu=nu, dimension=dim, time_stepSize=1e-3, No_of_gridpoint=(4 if les else 1) * n,
+                         method="RK4", LES_ON=1 if les else 0, LES_model=les, Cs=0.17, dtype="float64",
+                         parity_mode=not (dim == 2 and les))
+    if dim == 3:
+        initial_velocity(d, *random_spectrum_velocity(n, 4.0, 1.0, seed=2))
+    else:
+        initial_vorticity(d, gaussian_vorticity_2d(n, seed=2, kp=10.0))
+    d.U_hat1[...] = d.U_hat
+    ps = PlainSolver(n, dim, nu=nu, dt=1e-3, les=les, Cs=0.17, method="RK4", parity=not (dim == 2 and les),
+                     dtype=torch.float64, device="cuda")
+    Uh = d.U_hat.detach().to(torch.complex128).clone()
+    for _ in range(steps):
+        Uh = ps.step(Uh)
+        RK4_method.solveForNextTimestep(d)
+    d._plan.check()
+    assert _trel(d.U_hat, Uh) < 1e-11
+    del d, ps, Uh
+    torch.cuda.empty_cache()
