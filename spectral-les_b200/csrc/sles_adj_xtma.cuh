@@ -117,11 +117,14 @@ k_adj_xpass_tma(const __grid_constant__ AXTArgs<Tp> P) {
       }
     };
     // inverse x-transforms of a field and of i kx times it into slots s0, s0 + 3
-    auto inv2 = [&](C (&v)[V], int s0) {
+    // (after_release: a block barrier was just passed, the first transform
+    // skips its leading one)
+    auto inv2 = [&](C (&v)[V], int s0, bool after_release) {
       C b[V];
 #pragma unroll
       for (int m = 0; m < V; ++m) b[m] = cmuli_s(v[m], (Tp)kx_at(m));
-      fft.template run_tab<+1, true>(b, j, sm, W, twt);
+      if (after_release) fft.template run_tab<+1, true, 0, false>(b, j, sm, W, twt);
+      else fft.template run_tab<+1, true>(b, j, sm, W, twt);
       st(s0 + 3, b);
       fft.template run_tab<+1, true>(v, j, sm, W, twt);
       st(s0, v);
@@ -131,9 +134,9 @@ k_adj_xpass_tma(const __grid_constant__ AXTArgs<Tp> P) {
       for (int c = 0; c < 3; ++c) {
         C v[V], h[V];
         take(v);
-        fft.template run_tab<-1, true>(v, j, sm, W, twt);
+        fft.template run_tab<-1, true, 0, false>(v, j, sm, W, twt);
         take(h);
-        fft.template run_tab<-1, true>(h, j, sm, W, twt);
+        fft.template run_tab<-1, true, 0, false>(h, j, sm, W, twt);
         const C* pl = wait_at(t);
         const C* pu = P.need_ubar ? wait_at(t + 1) : nullptr;
         const C* pa = P.need_acc ? wait_at(t + 1 + P.need_ubar) : nullptr;
@@ -214,10 +217,10 @@ k_adj_xpass_tma(const __grid_constant__ AXTArgs<Tp> P) {
     for (int c = 0; c < 3; ++c) {
       C v[V];
       take(v);
-      inv2(v, c);
+      inv2(v, c, true);
 #pragma unroll
       for (int m = 0; m < V; ++m) v[m] = rst[rpos(c, m)];
-      inv2(v, 9 + c);
+      inv2(v, 9 + c, false);
     }
   }
 }

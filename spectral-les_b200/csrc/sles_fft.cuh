@@ -276,9 +276,11 @@ struct LineFFT {
   }
 
   // Transform with twiddles from `tab` (L entries, see fill_table); needs no init().
-  template <int DIR, bool LIN = false, int WS = 0>
+  // LEAD = false drops the leading barrier (the guard of the scratch against
+  // the previous transform's last reads) where the caller has just passed one.
+  template <int DIR, bool LIN = false, int WS = 0, bool LEAD = true>
   __device__ __forceinline__ void run_tab(C (&v)[V], int j, C* sm, int ws, const C* tab) {
-    if constexpr (S >= 2) lsync<WS>();
+    if constexpr (S >= 2 && LEAD) lsync<WS>();
     stage_tab<R0, DIR, S == 1, LIN>(v, tab, 1, j, sm, ws);
     if constexpr (S >= 2) {
       exchange<WS>(v, j, sm, ws);

@@ -647,14 +647,14 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
 #pragma unroll 1
       for (int c = 0; c < 3; ++c) {  // Y_c = Y(Z_c) - i ky Y(A2_c);  A1_c passes through
         take(v);
-        fft.template run_tab<-1>(v, j, sm, W, twt);
+        fft.template run_tab<-1, false, 0, false>(v, j, sm, W, twt);
         take(w);
-        fft.template run_tab<-1>(w, j, sm, W, twt);
+        fft.template run_tab<-1, false, 0, false>(w, j, sm, W, twt);
 #pragma unroll
         for (int m = 0; m < V; ++m) v[m] = cadd(v[m], cmuli_s(w[m], -kyv(m)));
         st(c, v);
         take(v);
-        fft.template run_tab<-1>(v, j, sm, W, twt);
+        fft.template run_tab<-1, false, 0, false>(v, j, sm, W, twt);
         st(3 + c, v);
       }
       continue;
@@ -670,12 +670,12 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
             take(v);
 #pragma unroll
             for (int m = 0; m < V; ++m) w[m] = cmuli_s(v[m], kyv(m));
-            fft.template run_tab<+1>(v, j, sm, W, twt);
+            fft.template run_tab<+1, false, 0, false>(v, j, sm, W, twt);
             st(sb + c, v);
             fft.template run_tab<+1>(w, j, sm, W, twt);
             st(sb + 6 + c, w);
             take(v);
-            fft.template run_tab<+1>(v, j, sm, W, twt);
+            fft.template run_tab<+1, false, 0, false>(v, j, sm, W, twt);
             st(sb + 3 + c, v);
           }
         }
@@ -683,7 +683,7 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
         take(v);  // A_w -> a_w and Ox = Y^-1(i ky A_w)
 #pragma unroll
         for (int m = 0; m < V; ++m) w[m] = cmuli_s(v[m], kyv(m));
-        fft.template run_tab<+1>(v, j, sm, W, twt);
+        fft.template run_tab<+1, false, 0, false>(v, j, sm, W, twt);
         st(2, v);
         fft.template run_tab<+1>(w, j, sm, W, twt);
         st(5, w);
@@ -691,15 +691,15 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
         take(w);
 #pragma unroll
         for (int m = 0; m < V; ++m) w[m] = csub(w[m], cmuli_s(v[m], kyv(m)));
-        fft.template run_tab<+1>(v, j, sm, W, twt);
+        fft.template run_tab<+1, false, 0, false>(v, j, sm, W, twt);
         st(0, v);
         fft.template run_tab<+1>(w, j, sm, W, twt);
         st(4, w);
         take(v);
-        fft.template run_tab<+1>(v, j, sm, W, twt);
+        fft.template run_tab<+1, false, 0, false>(v, j, sm, W, twt);
         st(1, v);
         take(v);
-        fft.template run_tab<+1>(v, j, sm, W, twt);
+        fft.template run_tab<+1, false, 0, false>(v, j, sm, W, twt);
         st(3, v);
       }
       continue;
@@ -709,7 +709,7 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
 #pragma unroll 1
       for (int c = 0; c < 3; ++c) {
         take(v);
-        fft.template run_tab<-1>(v, j, sm, W, twt);
+        fft.template run_tab<-1, false, 0, false>(v, j, sm, W, twt);
         st(c, v);
       }
       continue;
@@ -718,46 +718,46 @@ k_ypass(const __grid_constant__ YArgs<Tp> A) {
     C tt[V], acc[V], acc2[V];
     // G_x = N_x + 2i(ky F_xy + kz F_xz);  H_y = F_xy, H_z = F_xz, H_x = F_xx
     take(tt);
-    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    fft.template run_tab<-1, false, 0, false>(tt, j, sm, W, twt);
     st(4, tt);
 #pragma unroll
     for (int m = 0; m < V; ++m) acc[m] = cmuli_s(tt[m], (Tp)2 * kyv(m));
     take(tt);
-    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    fft.template run_tab<-1, false, 0, false>(tt, j, sm, W, twt);
     st(5, tt);
 #pragma unroll
     for (int m = 0; m < V; ++m) acc[m] = cadd(acc[m], cmuli_s(tt[m], kz2));
     take(tt);
-    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    fft.template run_tab<-1, false, 0, false>(tt, j, sm, W, twt);
 #pragma unroll
     for (int m = 0; m < V; ++m) tt[m] = cadd(tt[m], acc[m]);
     st(0, tt);
     take(tt);
-    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    fft.template run_tab<-1, false, 0, false>(tt, j, sm, W, twt);
     st(3, tt);
     // G_y = N_y + 2i(ky F_yy + kz F_yz);  G_z = N_z + 2i(ky F_yz + kz F_zz)
     take(tt);
-    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    fft.template run_tab<-1, false, 0, false>(tt, j, sm, W, twt);
 #pragma unroll
     for (int m = 0; m < V; ++m) acc[m] = cmuli_s(tt[m], (Tp)2 * kyv(m));
     take(tt);
-    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    fft.template run_tab<-1, false, 0, false>(tt, j, sm, W, twt);
 #pragma unroll
     for (int m = 0; m < V; ++m) {
       acc[m] = cadd(acc[m], cmuli_s(tt[m], kz2));
       acc2[m] = cmuli_s(tt[m], (Tp)2 * kyv(m));
     }
     take(tt);
-    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    fft.template run_tab<-1, false, 0, false>(tt, j, sm, W, twt);
 #pragma unroll
     for (int m = 0; m < V; ++m) tt[m] = cadd(tt[m], acc[m]);
     st(1, tt);
     take(tt);
-    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    fft.template run_tab<-1, false, 0, false>(tt, j, sm, W, twt);
 #pragma unroll
     for (int m = 0; m < V; ++m) acc2[m] = cadd(acc2[m], cmuli_s(tt[m], kz2));
     take(tt);
-    fft.template run_tab<-1>(tt, j, sm, W, twt);
+    fft.template run_tab<-1, false, 0, false>(tt, j, sm, W, twt);
 #pragma unroll
     for (int m = 0; m < V; ++m) tt[m] = cadd(tt[m], acc2[m]);
     st(2, tt);

@@ -161,23 +161,28 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
         for (int m = 0; m < V; ++m) ws[slot * fs + base + (j + T * m) * ps] = v[m];
       }
     };
-    // inverse x-transforms of component c of the new state (primes the next evaluation)
+    // inverse x-transforms of component c of the new state (primes the next
+    // evaluation); callers have just passed a block barrier (a tile release),
+    // so the first transform skips its leading one
     auto prep = [&](int c, C (&s)[V]) {
       if (LES) {
         C b[V];
 #pragma unroll
         for (int m = 0; m < V; ++m) b[m] = cmuli_s(s[m], (Tp)kx_at(m));  // i kx u_c
-        fft.template run_tab<+1, true>(b, j, sm, W, twt);
+        fft.template run_tab<+1, true, 0, false>(b, j, sm, W, twt);
         st(D + c, b);
+        fft.template run_tab<+1, true>(s, j, sm, W, twt);
       } else if (c >= 1) {
         C q[V];
         const Tp sg = (c == 2) ? (Tp)-1 : (Tp)1;  // -i kx w -> [3], i kx v -> [4]
 #pragma unroll
         for (int m = 0; m < V; ++m) q[m] = cmuli_s(s[m], sg * (Tp)kx_at(m));
-        fft.template run_tab<+1, true>(q, j, sm, W, twt);
+        fft.template run_tab<+1, true, 0, false>(q, j, sm, W, twt);
         st(c == 2 ? 3 : 4, q);
+        fft.template run_tab<+1, true>(s, j, sm, W, twt);
+      } else {
+        fft.template run_tab<+1, true, 0, false>(s, j, sm, W, twt);
       }
-      fft.template run_tab<+1, true>(s, j, sm, W, twt);
       st(c, s);
     };
     if (!A.fwd) {
@@ -196,11 +201,11 @@ k_xpass_tma(const __grid_constant__ XTArgs<Tp> P) {
     for (int c = 0; c < D; ++c) {
       C v[V];
       take(v);
-      fft.template run_tab<-1, true>(v, j, sm, W, twt);
+      fft.template run_tab<-1, true, 0, false>(v, j, sm, W, twt);
       if (LES) {  // + 2i kx F_cx
         C h[V];
         take(h);
-        fft.template run_tab<-1, true>(h, j, sm, W, twt);
+        fft.template run_tab<-1, true, 0, false>(h, j, sm, W, twt);
 #pragma unroll
         for (int m = 0; m < V; ++m) v[m] = cadd(v[m], cmuli_s(h[m], (Tp)(2 * kx_at(m))));
       }
