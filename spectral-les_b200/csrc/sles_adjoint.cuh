@@ -452,17 +452,19 @@ k_adj_zpass(const AZArgs<Tp> A) {
     for (int r = 0; r < 2; ++r) {
       const int f = grp + 12 * r;
       const int sbase = 9 * r, g = grp;  // slot base of the group; line index within it
-      const int s1 = (g < 9) ? sbase + g : -1, s2 = (g < 9) ? -1 : sbase + g - 9;  // d/dz = i kz a_c
+      // slot g, or for g >= 9 i kz times slot g - 9 (d/dz a_c), without
+      // branches that would split a warp's groups
+      const int sl = (g < 9) ? sbase + g : sbase + g - 9;
+      const Tp wr = (g < 9) ? (Tp)1 : (Tp)0, wk = (g < 9) ? (Tp)0 : (Tp)1;
       const C* sb = stage + buf * K::STAGE + ln * NKP;
       Tp* myreg = reg + (f * LPI + ln) * K::RS;
       C* sm = reinterpret_cast<C*>(myreg);
       C v[V];
       c2r_pre<F>(v, j, twN, [&](int k) {
-        C x = cmk<C>(0, 0);
-        if (!ok) return x;
-        if (s1 >= 0) x = sb[s1 * LPI * NKP + k];
-        else x = cmuli_s(sb[s2 * LPI * NKP + k], (Tp)k);
-        return x;
+        if (!ok) return cmk<C>(0, 0);
+        const C x = sb[sl * LPI * NKP + k];
+        const Tp kk = wk * (Tp)k;
+        return cmk<C>(wr * x.x - kk * x.y, wr * x.y + kk * x.x);
       });
       fft.template run<+1, WS>(v, j, sm, 1);
       F::template lsync<WS>();

@@ -998,6 +998,11 @@ k_zpass(const ZArgs<Tp> A) {
       s1 = 2; s2 = 0; sgn = -1;                               // omega = X^-1(i kx v) - i ky u
     }
   }
+  // the same without branches that split a warp's groups: the first term is
+  // (wr + i wk k) slot sa (wr, wk in {0, 1, sgn}); only the no-LES vorticity
+  // groups add a second slot
+  const int sa = (s1 >= 0) ? s1 : s2, s2b = (s1 >= 0) ? s2 : -1;
+  const Tp wr = (s1 >= 0) ? (Tp)1 : (Tp)0, wk = (s1 >= 0) ? (Tp)0 : sgn;
   const long long nbi = (A.nlines + LPI - 1) / LPI;
   // thread 0 stages the NIN input slots of line group `b` into buffer `buf`
   auto issue = [&](long long b, int buf) {
@@ -1025,10 +1030,11 @@ k_zpass(const ZArgs<Tp> A) {
       const C* sb = stage + buf * K::STAGE + ln * NKP;
       C v[V];
       c2r_pre<F>(v, j, twN, [&](int k) {
-        C r = cmk<C>(0, 0);
-        if (!ok) return r;
-        if (s1 >= 0) r = sb[s1 * K::SLOT_STRIDE + k];
-        if (s2 >= 0) r = cadd(r, cmuli_s(sb[s2 * K::SLOT_STRIDE + k], sgn * (Tp)k));
+        if (!ok) return cmk<C>(0, 0);
+        const C x = sb[sa * K::SLOT_STRIDE + k];
+        const Tp kk = wk * (Tp)k;
+        C r = cmk<C>(wr * x.x - kk * x.y, wr * x.y + kk * x.x);
+        if (s2b >= 0) r = cadd(r, cmuli_s(sb[s2b * K::SLOT_STRIDE + k], sgn * (Tp)k));
         return r;
       });
       fft.template run<+1, WS>(v, j, sm, 1);
