@@ -1044,40 +1044,53 @@ k_zpass(const ZArgs<Tp> A) {
       for (int m = 0; m < V; ++m) dst[F::pos(j, m)] = cscale(v[m], A.scale);
     }
     __syncthreads();
-    // ---- phase B: pointwise products
-    for (int p = tid; p < LPI * N; p += K::THREADS) {
-      const int pln = p / N, z = p % N;
+    // ---- phase B: pointwise products, two neighbouring points per thread
+    // (each field's pair moves as one 8/16-byte shared access)
+    for (int p = tid; p < LPI * N / 2; p += K::THREADS) {
+      const int pln = (2 * p) / N, z = (2 * p) % N;
       const long long pl = line0 + pln;
       if (pl >= A.nlines) continue;
       const long long o = pl * N + z;
-      Tp ub[3], cb[3];
-      const Tp* uo = nullptr;
-      const Tp* co = nullptr;
-      if (A.uphys) {
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) ub[c] = A.uphys[c * A.rs + o];
-        uo = ub;
-      }
-      if (A.cphys) {
-#pragma unroll
-        for (int c = 0; c < (DIM == 3 ? 3 : 1); ++c) cb[c] = A.cphys[c * A.rs + o];
-        co = cb;
-      }
       const int sp = pln * K::RS + z;
-      if (A.umax) {
+      Tp loc[2 * K::NG];  // [field][point]
 #pragma unroll
-        for (int c = 0; c < DIM; ++c) lmax = fmax(lmax, (double)(uo ? uo[c] : reg[c * SFS + sp]));
+      for (int f = 0; f < K::NG; ++f) {
+        const C x = *reinterpret_cast<const C*>(reg + f * SFS + sp);
+        loc[2 * f] = x.x;
+        loc[2 * f + 1] = x.y;
       }
       Tp cdx2 = A.cdx2;
       if (LES && A.mcs) {  // the member's C_s (the host's float64 products, rounded once)
         const double cs = A.mcs[pl / A.lpm];
         cdx2 = A.vreman ? (Tp)(2.5 * cs * cs * A.dx * A.dx) : (Tp)((cs * A.dx) * (cs * A.dx));
       }
-      z_pointwise<Tp, DIM, LES, MODEL, PAR2D>(reg, SFS, sp, uo, co, cdx2);
-      if (A.stress_only) {
 #pragma unroll
-        for (int c = 0; c < DIM; ++c) reg[c * SFS + sp] = (Tp)0;
+      for (int q = 0; q < 2; ++q) {
+        Tp ub[3], cb[3];
+        const Tp* uo = nullptr;
+        const Tp* co = nullptr;
+        if (A.uphys) {
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) ub[c] = A.uphys[c * A.rs + o + q];
+          uo = ub;
+        }
+        if (A.cphys) {
+#pragma unroll
+          for (int c = 0; c < (DIM == 3 ? 3 : 1); ++c) cb[c] = A.cphys[c * A.rs + o + q];
+          co = cb;
+        }
+        if (A.umax) {
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) lmax = fmax(lmax, (double)(uo ? uo[c] : loc[2 * c + q]));
+        }
+        z_pointwise<Tp, DIM, LES, MODEL, PAR2D>(loc, 2, q, uo, co, cdx2);
+        if (A.stress_only) {
+#pragma unroll
+          for (int c = 0; c < DIM; ++c) loc[2 * c + q] = (Tp)0;
+        }
       }
+#pragma unroll
+      for (int f = 0; f < K::NOUT; ++f) *reinterpret_cast<C*>(reg + f * SFS + sp) = cmk<C>(loc[2 * f], loc[2 * f + 1]);
     }
     __syncthreads();
     // ---- phase C: r2c of product `grp` (with block-wide line barriers, groups
