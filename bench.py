@@ -738,7 +738,8 @@ def bench_zoo(rank):
     (Smagorinsky RK3 on every x variant, Vreman corrected ETD2, no-LES RK4,
     the alternative y/z variants), the FP64 passes, the 2D passes at 1024^2,
     the standalone transforms and diagnostics, the device-dt controller, the
-    adjoint passes at 64^3, a slab decomposition and a member batch."""
+    adjoint passes at 64^3 and 128^3 (direct-load and TMA-ring x passes), a
+    slab decomposition and a member batch."""
     import torch
     from sles import ETD2_method, RK3_method, RK4_method, diagnostics
     from sles import _native as nat
@@ -807,13 +808,14 @@ def bench_zoo(rank):
     del d
     release()
     done.append("device-dt controller at 64^3")
-    ro = RK4Rollout(64, 1e-3, 1e-3, les="Smagorinsky", Cs=0.17, dtype=torch.float32, checkpoint_every=2)
-    U0 = make_domain(64, "float32", rank, method="RK4").U_hat.clone().to(ro.cdtype)
-    UT, ck = ro.forward_states(U0, 0.17, 2)
-    ro.backward_states(ck, UT[..., : ro.nk].clone(), 0.17, 2)
-    del ro, U0, UT, ck
-    release()
-    done.append("adjoint rk4 at 64^3")
+    for na in (64, 128):  # direct-load adjoint x pass at 64^3, the TMA-ring one at 128^3
+        ro = RK4Rollout(na, 1e-3, 1e-3, les="Smagorinsky", Cs=0.17, dtype=torch.float32, checkpoint_every=2)
+        U0 = make_domain(na, "float32", rank, method="RK4").U_hat.clone().to(ro.cdtype)
+        UT, ck = ro.forward_states(U0, 0.17, 2)
+        ro.backward_states(ck, UT[..., : ro.nk].clone(), 0.17, 2)
+        del ro, U0, UT, ck
+        release()
+        done.append("adjoint rk4 at %d^3" % na)
     base = make_domain(256, "float32", rank)
     doms = [SlabDomain(256, nu=NU, dt=DT, method="RK3", les="Smagorinsky", Cs=CS, dtype=torch.float32, nranks=2,
                        rank=r, exchange=lambda o, i: None) for r in range(2)]
