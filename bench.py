@@ -890,7 +890,7 @@ def bench_steps(case, n, precision, steps, warmup, rank, xvar=-1):
             "x_variant": d._plan.get_variant(0)}
 
 
-def north_star_summary(out):
+def headline_summary(out):
     """The headline figures in a few hundred characters (printed last)."""
     r = lambda x, k=4: None if x is None else (round(x, k) if isinstance(x, float) else x)
     ns = {"fp32_256": out["value"], "roofline_frac": out["roofline"]["frac"],
@@ -1142,7 +1142,7 @@ def main():
         if "fp64" in out:  # precision-matched: the fused float64 path against the float64 CPU port
             out["fp64"]["fused_fp64_vs_cpu_fp64"] = round(out["fp64"]["fused_fp64_value"] / v_cpu, 1)
     out["clocks"] = clk.summary()
-    out["north_star"] = north_star_summary(out)  # last: the compact figures stay in a short stdout tail
+    out["headline"] = headline_summary(out)  # last: the compact figures stay in a short stdout tail
     if rank == 0:
         print(json.dumps(out))
     if world > 1:
