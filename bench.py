@@ -698,6 +698,95 @@ def ensemble_members(seed):
     return members
 
 
+def bench_slab(rank, n=512, nranks=(2, 4), steps=3):
+    """The slab decomposition's compute on one GPU: the P ranks of one 512^3
+    FP32 Smagorinsky RK3 domain run one after another in one process (their
+    all-to-alls as copies between their buffers, outside the timed calls).
+    Each rank's own kernel time per step (CUDA events around its prime,
+    middle and stage calls) against the whole-grid fused step, and the bytes
+    each rank sends per step through the two exchanges of every RHS
+    evaluation.  The projected multi-GPU step (the slowest rank's compute plus
+    its exchange bytes at the measured 770 GB/s per direction of a peer copy,
+    not overlapped) is a model, not a measurement."""
+    import torch
+    from sles import RK3_method
+    from sles.slab import SlabDomain
+    d = make_domain(n, "float32", rank)
+    U = d.U_hat.clone()
+    whole = time_steps(d, steps, RK3_method.solveForNextTimestep)
+    del d
+    torch.cuda.empty_cache()
+    out = {"n": n, "whole_grid_ms_per_step": round(whole / steps * 1e3, 3)}
+    st = torch.cuda.current_stream()
+    for P in nranks:
+        doms = [SlabDomain(n, nu=NU, dt=DT, method="RK3", les="Smagorinsky", Cs=CS, dtype=torch.float32, nranks=P,
+                           rank=r, exchange=lambda o, i: None) for r in range(P)]
+        for s in doms:
+            s.set_state(U)
+        ms = [0.0] * P
+
+        def timed(r, fn):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            return (e0, e1, r)
+
+        def copy(attr_s, attr_r, nf):
+            for q in range(P):
+                for r in range(P):
+                    b = doms[0].block
+                    for f in range(nf):
+                        getattr(doms[q], attr_r)[f, r * b:(r + 1) * b].copy_(getattr(doms[r], attr_s)[f, q * b:(q + 1) * b])
+
+        evs = []
+        for k in range(steps + 1):  # the first step is a warm-up
+            bufs = [(s.U_hat, s._u0) for s in doms]
+            for s in doms:
+                s._umax.zero_()
+            for rk in range(3):
+                for r, (s, (A, B)) in enumerate(zip(doms, bufs)):
+                    cur = A if rk == 0 else B
+                    if s._primed != (cur.data_ptr(), cur._version):
+                        evs.append(timed(r, lambda s=s, cur=cur: s.plan.slab_prime(cur)))
+                copy("send1", "recv1", doms[0].n1)
+                for r, s in enumerate(doms):
+                    evs.append(timed(r, lambda s=s, rk=rk: s.plan.slab_middle(s._umax if rk == 0 else None)))
+                copy("send2", "recv2", doms[0].n2)
+                for r, (s, (A, B)) in enumerate(zip(doms, bufs)):
+                    cur = A if rk == 0 else B
+                    evs.append(timed(r, lambda s=s, rk=rk, cur=cur, A=A, B=B:
+                                     s.plan.slab_stage(rk, s.dt, cur, A, None, B, None, 0)))
+                    s._primed = (B.data_ptr(), B._version)
+            for s, (A, B) in zip(doms, bufs):
+                s.U_hat, s._u0 = B, A
+                s._primed = (B.data_ptr(), B._version)
+            if k == 0:
+                torch.cuda.synchronize()
+                evs = []
+        torch.cuda.synchronize()
+        for e0, e1, r in evs:
+            ms[r] += e0.elapsed_time(e1)
+        for s in doms:
+            s.check()
+        esz = 8
+        sent = 3 * (doms[0].n1 + doms[0].n2) * (P - 1) * doms[0].block * esz  # bytes per rank per step
+        comp = max(ms) / steps
+        proj = comp + sent / 770e9 * 1e3
+        out["P%d" % P] = {"per_rank_compute_ms_per_step": [round(m / steps, 3) for m in ms],
+                          "compute_efficiency_vs_whole_grid": round(whole / steps * 1e3 / (P * comp), 3),
+                          "exchange_bytes_per_rank_per_step": sent,
+                          "model_exchange_ms_at_770GBs": round(sent / 770e9 * 1e3, 3),
+                          "model_step_ms_no_overlap": round(proj, 3),
+                          "model_value_no_overlap": round(float(n) ** 3 / (proj * 1e-3) / 1e6, 1)}
+        del doms
+        torch.cuda.empty_cache()
+    out["unit"] = UNIT
+    out["note"] = ("ranks emulated one after another on one GPU; the exchange time is modelled from the bytes, "
+                   "not measured")
+    return out
+
+
 def bench_ensemble(rank, steps=200):
     """The 48-member ensemble: one captured graph per PERIOD steps (each member
     a stream branch) against the same members stepped one at a time."""
@@ -917,6 +1006,9 @@ def headline_summary(out):
         ns["adjoint_cs_rel_err"] = r(out["adjoint"]["cs_rel_err_f64_vs_richardson"], 12)
     if "ensemble" in out:
         ns["ensemble_x_seq"] = out["ensemble"]["speedup_vs_sequential"]
+    if "slab" in out:
+        ns["slab512_compute_eff"] = {k: v["compute_efficiency_vs_whole_grid"] for k, v in out["slab"].items()
+                                     if isinstance(v, dict)}
     if "fft_vs_cufft" in out:
         ns["fft_r2c_x_cufft"] = {k: v["speedup_r2c_vs_cufft"] for k, v in out["fft_vs_cufft"].items()
                                  if isinstance(v, dict)}
@@ -934,7 +1026,7 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (use the default or cached kernel variants)")
-    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble", "driver", "fft", "steps", "kernels", "zoo",
+    ap.add_argument("--only", choices=["n512", "adjoint", "ensemble", "driver", "fft", "steps", "kernels", "zoo", "slab",
                                        "cfg2"],
                     help="run one extra block alone and print it (profiling; not a bench line); 'steps': "
                          "--case at --n stepped --steps times after --warmup (for ncu launch lists)")
@@ -976,6 +1068,7 @@ def main():
     if args.only:
         peak, _ = measured_peak()
         fn = {"n512": lambda: bench_512(peak, rank), "adjoint": lambda: bench_adjoint(rank),
+              "slab": lambda: bench_slab(rank),
               "ensemble": lambda: bench_ensemble(rank), "driver": lambda: bench_driver(rank),
               "fft": lambda: bench_fft(rank),
               "kernels": lambda: bench_kernels(args.case, args.n, args.precision, rank, args.xvar),
@@ -1124,6 +1217,7 @@ def main():
         out["cfg2_error_history"] = bench_cfg2_history(rank)
         out["fft_vs_cufft"] = bench_fft(rank)
         out["n512"] = bench_512(peak, rank)
+        out["slab"] = bench_slab(rank)
         adj = bench_adjoint(rank)
         out["adjoint"] = adj
         out["adjoint_fwd_ratio"] = adj["adjoint_fwd_ratio"]
