@@ -839,7 +839,11 @@ struct ZGeo {
   static constexpr int NOUT = (DIM == 3) ? (LES ? 9 : 3) : (LES ? (PAR2D ? 4 : 5) : 2);
   static constexpr int NKP = ((N / 2 + 1) + 3) / 4 * 4;
   static constexpr int THREADS = NG * LPI * T;
-  static constexpr int MINB = (sizeof(Tp) == 4) ? (THREADS <= 192 ? 3 : (THREADS <= 256 ? 2 : 1)) : 1;
+  // float32: 3 blocks per SM for one line per item (a 512 line's 192 threads
+  // included), 2 for several lines up to 256 threads (their registers as one
+  // line's), else 1
+  static constexpr int MINB =
+      (sizeof(Tp) == 4) ? ((THREADS <= 192 && LPI == 1) || THREADS <= 96 ? 3 : (THREADS <= 256 ? 2 : 1)) : 1;
   // per (field, line) region: the line's FFT exchange scratch (LS complex,
   // LS = 8 mod 16 keeps the autosort writes conflict-free) and, between the
   // transforms, the physical line itself (N reals)
