@@ -406,6 +406,15 @@ int sles_selftest_wait_timeout(sles_plan* plan, void* stream);
 /* The same self-test against any device error word (e.g. an adjoint
  * workspace's header; 4-byte aligned device pointer). */
 int sles_selftest_wait_timeout_word(void* word_dev, void* stream);
+/*
+ * Device copy of `height` rows of `width` bytes, rows `src_pitch` /
+ * `dst_pitch` bytes apart (all three multiples of 8, both pointers 8-byte
+ * aligned device memory), on `stream`: fields between the padded layout
+ * (rows of nkp bins) and the reference's contiguous (..., N//2+1) layout,
+ * e.g. around host copies.  No counterpart in the reference.
+ */
+int sles_copy_rows(void* dst, size_t dst_pitch, const void* src, size_t src_pitch, size_t width, size_t height,
+                   void* stream);
 /* Human-readable text for a status code (static storage). */
 const char* sles_status_string(int status);
 int sles_version(void);

@@ -350,6 +350,20 @@ int sles_slab_stage(sles_plan* p, int stage, double dt, const void* ucur, const 
   return p->eng->slab_stage(p->info, stage, dt, ucur, u0, u1, uout, aux, flags, (cudaStream_t)stream);
 }
 
+int sles_copy_rows(void* dst, size_t dst_pitch, const void* src, size_t src_pitch, size_t width, size_t height,
+                   void* stream) {
+  if (!dst || !src || width > dst_pitch || width > src_pitch) return SLES_ERR_INVALID_ARG;
+  if ((dst_pitch | src_pitch | width) % 8 != 0 || ((uintptr_t)dst | (uintptr_t)src) % 8 != 0)
+    return SLES_ERR_INVALID_ARG;
+  if (width == 0 || height == 0) return SLES_OK;
+  if (width / 8 > 0x7fffffffULL) return SLES_ERR_UNSUPPORTED;
+  constexpr int ROWS = 8;  // rows (warps) per block
+  return sles::launch(sles::k_copy_rows8, (long long)((height + ROWS - 1) / ROWS), 32 * ROWS, 0,
+                      (cudaStream_t)stream, reinterpret_cast<unsigned long long*>(dst), (long long)(dst_pitch / 8),
+                      reinterpret_cast<const unsigned long long*>(src), (long long)(src_pitch / 8), (int)(width / 8),
+                      (long long)height);
+}
+
 int sles_selftest_wait_timeout_word(void* word, void* stream) {
   if (!word || ((uintptr_t)word) % sizeof(unsigned) != 0) return SLES_ERR_INVALID_ARG;
   return sles::launch(sles::k_wait_selftest, 1, 32, 0, (cudaStream_t)stream, reinterpret_cast<unsigned*>(word),

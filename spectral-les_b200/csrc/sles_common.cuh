@@ -91,6 +91,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
 
 // Self-test of the timeout path: waits on an mbarrier that nothing arrives
 // at; the bounded wait gives up after `limit` polls and raises the flag.
+// Rows of `w` 8-byte words from src (row pitch sp) to dst (row pitch dp),
+// one warp per row (coalesced row segments): padded <-> contiguous fields.
+static __global__ void k_copy_rows8(unsigned long long* __restrict__ dst, long long dp,
+                                   const unsigned long long* __restrict__ src, long long sp, int w, long long h) {
+  const long long row = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (row >= h) return;
+  const unsigned long long* s = src + row * sp;
+  unsigned long long* d = dst + row * dp;
+  for (int c = threadIdx.x & 31; c < w; c += 32) d[c] = s[c];
+}
+
 static __global__ void k_wait_selftest(unsigned* flag, long limit) {
   __shared__ uint64_t bar;
   if (threadIdx.x == 0) {

@@ -30,7 +30,7 @@ EXPORTED = [
     "sles_plan_check", "sles_selftest_wait_timeout", "sles_selftest_wait_timeout_word", "sles_adjoint_check",
     "sles_static_workspace_check", "sles_static_workspace_selftest_timeout",
     "sles_plan_set_slab", "sles_plan_set_batch", "sles_slab_info", "sles_slab_buffers", "sles_slab_prime", "sles_slab_middle",
-    "sles_slab_stage",
+    "sles_slab_stage", "sles_copy_rows",
 ]
 DT_DONE, DT_SNAPSHOT, DT_NAN, DT_TOO_SMALL = 1, 2, 4, 8
 
@@ -122,6 +122,7 @@ def load_library(path: str = LIB_PATH):
         "sles_slab_prime": (i, [vp, vp, vp]),
         "sles_slab_middle": (i, [vp, vp, vp]),
         "sles_slab_stage": (i, [vp, i, d, vp, vp, vp, vp, vp, i, vp]),
+        "sles_copy_rows": (i, [vp, ctypes.c_size_t, vp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, vp]),
         "sles_adjoint_workspace_bytes": (ctypes.c_size_t, [vp]),
         "sles_adjoint_seed": (i, [vp, vp, d, vp, vp, vp, vp]),
         "sles_adjoint_prime": (i, [vp, vp, vp, vp, vp]),
@@ -138,6 +139,17 @@ def load_library(path: str = LIB_PATH):
 def check(status, where):
     if status != 0:
         raise SlesError(status, where)
+
+
+def copy_rows(dst, src, width, height, dst_pitch, src_pitch, stream=None):
+    """sles_copy_rows: ``height`` rows of ``width`` bytes between device
+    tensors, rows ``dst_pitch`` / ``src_pitch`` bytes apart (padded <->
+    contiguous fields), on ``stream`` (default: the current stream)."""
+    L = load_library()
+    s = stream if stream is not None else torch.cuda.current_stream(dst.device)
+    check(L.sles_copy_rows(ctypes.c_void_p(dst.data_ptr()), int(dst_pitch), ctypes.c_void_p(src.data_ptr()),
+                           int(src_pitch), int(width), int(height), ctypes.c_void_p(s.cuda_stream)),
+          "sles_copy_rows")
 
 
 def ptr(t):

@@ -21,6 +21,7 @@ from __future__ import annotations
 import torch
 
 from . import ETD2_method, RK3_method, RK4_method
+from . import _native as nat
 
 __all__ = ["HostStepper"]
 
@@ -35,6 +36,9 @@ class HostStepper:
         shape, dt, dev = tuple(domain.U_hat.shape), domain.U_hat.dtype, domain.device
         self.din = [torch.empty(shape, dtype=dt, device=dev) for _ in range(2)]
         self.dout = [torch.empty(shape, dtype=dt, device=dev) for _ in range(2)]
+        esz = torch.empty((), dtype=dt).element_size()
+        # staging buffers [..][nk] <-> padded state [..][nkp]: rows copied by sles_copy_rows
+        self._rowcopy = (domain._nk * esz, int(torch.Size(shape).numel()) // domain._nk, domain._nkp * esz)
         self.h2d = torch.cuda.Stream(dev)
         self.d2h = torch.cuda.Stream(dev)
         ev = lambda: [torch.cuda.Event() for _ in range(2)]
@@ -59,10 +63,12 @@ class HostStepper:
                 self.din[b].copy_(hi, non_blocking=True)
                 self.in_ready[b].record(self.h2d)
             cur.wait_event(self.in_ready[b])
-            d.U_hat.copy_(self.din[b])
+            w, rows, pitch = self._rowcopy
+            nat.copy_rows(d._s_uhat, self.din[b], w, rows, pitch, w, cur)
             if d.method in ("RK4", "ETD2"):            # RK4, or ETD2's RK4 bootstrap step:
-                d.U_hat1.copy_(self.din[b])            # U_hat1 = U_hat on entry (SM_solver.py:33)
+                nat.copy_rows(d._s_u1, self.din[b], w, rows, pitch, w, cur)  # U_hat1 = U_hat (SM_solver.py:33)
             d._mark_stepped()                          # stage 0 derives U and curl from this U_hat
+            d._primed = None                           # a raw copy: the workspace holds no x inverse of it
             if d.method == "ETD2":
                 d.firstIteration = True                # each item starts its own ETD2 history
             self.in_free[b].record(cur)
@@ -70,7 +76,7 @@ class HostStepper:
                 step(d)
             if self._used[b]:
                 cur.wait_event(self.out_free[b])      # the host copy of dout[b] is done
-            self.dout[b].copy_(d.U_hat)
+            nat.copy_rows(self.dout[b], d._s_uhat, w, rows, w, pitch, cur)
             self.out_ready[b].record(cur)
             self.d2h.wait_event(self.out_ready[b])
             with torch.cuda.stream(self.d2h):
